@@ -1,0 +1,227 @@
+/*
+ * matrox_b200.h -- C-ABI of the B200 (sm_100a) evaluator of Y = K~ W for HSS and H2-b
+ * compressed kernel matrices in MatRox's compressed data storage (CDS).
+ *
+ * Two groups of entry points:
+ *
+ * 1. Drop-ins with the reference's own signatures.  They take HOST arrays exactly as
+ *    the reference's generated or structure-generic evaluators do, copy what is needed
+ *    to the GPU, evaluate there and copy `apres` back before returning.  The device
+ *    copy of the CDS is cached between calls (see mxb_cache_invalidate).  On entry,
+ *    `wskel` is ignored and `uskel` is not read; on return neither workspace is written
+ *    unless MXB_FLAG_MIRROR_WORKSPACES is set (mxb_set_flags).  Unlike the reference they
+ *    return 0 on success and a negative MXB_ERR_* code on failure (message in
+ *    mxb_last_error()).
+ *
+ * 2. A plan API on DEVICE pointers (mxb_plan_*), used by the Python binding, the
+ *    torch.autograd.Function and the benchmarks: the CDS is uploaded once, every
+ *    evaluation is a handful of kernel launches on a caller stream.
+ *
+ * Array conventions (all from the reference): column-major blocks; D / B / VT hold the
+ * near blocks, far couplings and projections at element offsets Dptr / Bptr (uint64) and
+ * VTptr (int32); W ("mrhs") and Y ("apres") are leaf-blocked: leaf i owns a Ddim[i] x nrhs
+ * column-major block at element offset wptr[i] / uptr[i]; lchildren[v] == -1 marks a leaf.
+ */
+#ifndef MATROX_B200_H
+#define MATROX_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define MXB_API __attribute__((visibility("default")))
+#else
+#define MXB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------------- */
+#define MXB_OK 0
+#define MXB_ERR_ARG (-1)        /* null pointer, negative size, bad mode               */
+#define MXB_ERR_STRUCTURE (-2)  /* index out of range, cycle, rank/size inconsistency  */
+#define MXB_ERR_CUDA (-3)       /* CUDA runtime error (message has the CUDA string)    */
+#define MXB_ERR_NOMEM (-4)      /* device or host allocation failed                    */
+#define MXB_ERR_TIMEOUT (-5)    /* a bounded device-side wait gave up                  */
+#define MXB_ERR_UNSUPPORTED (-6)/* shape outside what a kernel variant supports        */
+
+/* ---- precision modes --------------------------------------------------------------- */
+#define MXB_PREC_FP64 0       /* FP64 everywhere (reference mode)                        */
+#define MXB_PREC_SPLIT_BF16 1 /* near/far on BF16 tensor cores with hi+lo split operands,
+                                 FP32 accumulation; transfers FP32; FP64 final Y        */
+
+/* ---- flags for the drop-ins ---------------------------------------------------------- */
+#define MXB_FLAG_MIRROR_WORKSPACES 1u /* copy wskel/uskel back to the caller's arrays    */
+#define MXB_FLAG_OUTPUT_IS_ZERO 2u    /* caller guarantees apres == 0 on entry (H2-b):
+                                         skip its upload                                */
+
+/* ---- library state ------------------------------------------------------------------- */
+MXB_API const char *mxb_last_error(void);
+MXB_API const char *mxb_version(void);
+/* Precision used by the drop-ins (default MXB_PREC_FP64). */
+MXB_API int32_t mxb_set_precision(int32_t mode);
+MXB_API int32_t mxb_set_flags(uint32_t flags);
+/* Drop every cached device copy of a CDS (required after changing CDS values in place). */
+MXB_API int32_t mxb_cache_invalidate(void);
+
+/* ---- drop-ins: H2-b -------------------------------------------------------------------- */
+
+/* Replaces CBHGEMM, codeGen/H2GEMM.h:380-389 (coarsened + blocked H2-b evaluation).
+ * ncount / fcount are the numbers of near / far block ROWS (nblockSet has ncount+1
+ * entries, fblockSet fcount+1); cdepth is the number of coarsened levels. */
+MXB_API int32_t CBHGEMM(double *D, double *B, double *VT, uint64_t *Dptr, uint64_t *Bptr,
+                int32_t *VTptr, int32_t *lchildren, int32_t *rchildren, int32_t *levelset,
+                int32_t *idx, double *mrhs, double *apres, int32_t nrhs, int32_t *Ddim,
+                int32_t *wptr, int32_t *uptr, double *wskel, int32_t *wskeloffset,
+                double *uskel, int32_t *uskeloffset, int32_t *lm, int32_t *slen,
+                int32_t *nblockSet, int32_t *nblocks, int32_t *npairx, int32_t *npairy,
+                int32_t *fblockSet, int32_t *fblocks, int32_t *fpairx, int32_t *fpairy,
+                int32_t ncount, int32_t fcount, int32_t *wpart, int32_t *clevelset,
+                int cdepth);
+
+/* Replaces lowH2GEMM, codeGen/H2GEMM.h:506-515 (same arguments and result as CBHGEMM). */
+MXB_API int32_t lowH2GEMM(double *D, double *B, double *VT, uint64_t *Dptr, uint64_t *Bptr,
+                  int32_t *VTptr, int32_t *lchildren, int32_t *rchildren, int32_t *levelset,
+                  int32_t *idx, double *mrhs, double *apres, int32_t nrhs, int32_t *Ddim,
+                  int32_t *wptr, int32_t *uptr, double *wskel, int32_t *wskeloffset,
+                  double *uskel, int32_t *uskeloffset, int32_t *lm, int32_t *slen,
+                  int32_t *nblockSet, int32_t *nblocks, int32_t *npairx, int32_t *npairy,
+                  int32_t *fblockSet, int32_t *fblocks, int32_t *fpairx, int32_t *fpairy,
+                  int32_t ncount, int32_t fcount, int32_t *wpart, int32_t *clevelset,
+                  int cdepth);
+
+/* Replaces blockGEMM, codeGen/H2GEMM.h:255-262 (blocked H2-b over uncoarsened level sets;
+ * levelset / idx are top-down, depth levels, root excluded). */
+MXB_API int32_t blockGEMM(double *D, double *B, double *VT, uint64_t *Dptr, uint64_t *Bptr,
+                  int32_t *VTptr, int32_t *lchildren, int32_t *rchildren, int32_t *levelset,
+                  int32_t *idx, double *mrhs, double *apres, int32_t nrhs, int32_t *Ddim,
+                  int32_t *wptr, int32_t *uptr, double *wskel, int32_t *wskeloffset,
+                  double *uskel, int32_t *uskeloffset, int32_t *lm, int32_t *slen,
+                  int32_t *nblockSet, int32_t *nblocks, int32_t *npairx, int32_t *npairy,
+                  int32_t *fblockSet, int32_t *fblocks, int32_t *fpairx, int32_t *fpairy,
+                  int32_t ncount, int32_t fcount, int32_t depth);
+
+/* Replaces the generated H2-b evaluator HGEMM, symGen/HGEMM_gen.h:120-124.  The generated
+ * code bakes the number of near block rows, far block rows and coarsened levels into its
+ * loop bounds; here they are set once with mxb_hgemm_set_shape (nrow, frow, cdepth as in
+ * CBHGEMM's ncount, fcount, cdepth). */
+MXB_API int32_t mxb_hgemm_set_shape(int32_t nrow, int32_t frow, int32_t cdepth);
+MXB_API int32_t HGEMM(double *D, double *B, double *VT, uint64_t *Dptr, uint64_t *Bptr,
+              int32_t *VTptr, int32_t *lchildren, int32_t *rchildren, int32_t *levelset,
+              int32_t *idx, double *mrhs, double *apres, int32_t nrhs, int32_t *Ddim,
+              int32_t *wptr, int32_t *uptr, double *wskel, int32_t *wskeloffset,
+              double *uskel, int32_t *uskeloffset, int32_t *lm, int32_t *slen,
+              int32_t *nblockSet, int32_t *nblocks, int32_t *npairx, int32_t *npairy,
+              int32_t *fblockSet, int32_t *fblocks, int32_t *fpairx, int32_t *fpairy,
+              int32_t *wpart, int32_t *clevelset);
+
+/* ---- drop-ins: HSS ----------------------------------------------------------------------- */
+
+/* Replaces parHSSGEMM, codeGen/HSSGEMM.h:131-134: ncount = number of leaves,
+ * fcount = numnodes - 1 (far couplings are sibling pairs, B of node i at Bptr[i-1]). */
+MXB_API int32_t parHSSGEMM(double *D, double *B, double *VT, uint64_t *Dptr, uint64_t *Bptr,
+                   int32_t *VTptr, int32_t *lchildren, int32_t *rchildren, int32_t *levelset,
+                   int32_t *idx, double *mrhs, double *apres, int32_t nrhs, int32_t *Ddim,
+                   int32_t *wptr, int32_t *uptr, double *wskel, int32_t *wskeloffset,
+                   double *uskel, int32_t *uskeloffset, int32_t *lm, int32_t *slen,
+                   int32_t *wpart, int32_t *clevelset, int ncount, int fcount, int cdepth);
+
+/* Replaces lowHSSGEMM, codeGen/HSSGEMM.h:246-249 (same arguments and result). */
+MXB_API int32_t lowHSSGEMM(double *D, double *B, double *VT, uint64_t *Dptr, uint64_t *Bptr,
+                   int32_t *VTptr, int32_t *lchildren, int32_t *rchildren, int32_t *levelset,
+                   int32_t *idx, double *mrhs, double *apres, int32_t nrhs, int32_t *Ddim,
+                   int32_t *wptr, int32_t *uptr, double *wskel, int32_t *wskeloffset,
+                   double *uskel, int32_t *uskeloffset, int32_t *lm, int32_t *slen,
+                   int32_t *wpart, int32_t *clevelset, int ncount, int fcount, int cdepth);
+
+/* Replaces seqHSSGEMM, codeGen/HSSGEMM.h:18-21 (levelset / idx top-down, depth levels). */
+MXB_API int32_t seqHSSGEMM(double *D, double *B, double *VT, uint64_t *Dptr, uint64_t *Bptr,
+                   int32_t *VTptr, int32_t *lchildren, int32_t *rchildren, int32_t *levelset,
+                   int32_t *idx, double *mrhs, double *apres, int32_t nrhs, int32_t *Ddim,
+                   int32_t *wptr, int32_t *uptr, double *wskel, int32_t *wskeloffset,
+                   double *uskel, int32_t *uskeloffset, int32_t *lm, int32_t *slen,
+                   int32_t ncount, int32_t fcount, int32_t depth);
+
+/* Replaces the generated HSS evaluator (codeGen/HGEMM_gen.h:120-124, exported there as
+ * HGEMM; renamed here so both generated forms can live in one library).  nleaf / numnodes
+ * / cdepth come from mxb_hgemm_hss_set_shape. */
+MXB_API int32_t mxb_hgemm_hss_set_shape(int32_t nleaf, int32_t cdepth);
+MXB_API int32_t HGEMM_HSS(double *D, double *B, double *VT, uint64_t *Dptr, uint64_t *Bptr,
+                  int32_t *VTptr, int32_t *lchildren, int32_t *rchildren, int32_t *levelset,
+                  int32_t *idx, double *mrhs, double *apres, int32_t nrhs, int32_t *Ddim,
+                  int32_t *wptr, int32_t *uptr, double *wskel, int32_t *wskeloffset,
+                  double *uskel, int32_t *uskeloffset, int32_t *lm, int32_t *slen,
+                  int32_t *wpart, int32_t *clevelset);
+
+/* ---- input / output permutation (matroxTest-V1/hcds.h:766-788 `transform`) -------------- */
+
+/* TW[leaf-blocked] = W[perm rows]: W is n x nrhs column-major (ldw >= n) in the original
+ * point order; perm[t] is the original row of tree position t; leaf i owns tree positions
+ * [leafofs[i], leafofs[i+1]) and its block starts at TW + wptr[i] with leading dimension
+ * leafofs[i+1]-leafofs[i].  Host pointers, synchronous. */
+MXB_API int32_t mxb_transform(const int32_t *perm, const int32_t *leafofs, const int32_t *wptr,
+                      int32_t nleaf, const double *W, int64_t n, int64_t ldw, int32_t nrhs,
+                      double *TW);
+/* Inverse: Y[perm rows] = TY[leaf-blocked] (the reference has no inverse; its output stays
+ * in tree order, matroxTest-V1/Util.h:320). */
+MXB_API int32_t mxb_untransform(const int32_t *perm, const int32_t *leafofs, const int32_t *uptr,
+                        int32_t nleaf, const double *TY, int64_t n, int64_t ldy, int32_t nrhs,
+                        double *Y);
+
+/* Device-pointer form of both directions, asynchronous on `stream`.  direction 0:
+ * dst(leaf-blocked) = src[perm rows]; direction 1: dst[perm rows] (+)= src(leaf-blocked).
+ * The caller-order matrix has element (p, j) at p*row_stride + j*col_stride (row-major
+ * (N, r): row_stride = r, col_stride = 1; column-major: 1, ld).  d_blockofs[i] is the
+ * element offset of leaf i's block (Ddim[i] x nrhs, column-major). */
+MXB_API int32_t mxb_permute_rows(const int32_t *d_perm, const int32_t *d_leafofs, const int32_t *d_blockofs,
+                         int32_t nleaf, int64_t n, const double *src, double *dst, int64_t row_stride,
+                         int64_t col_stride, int32_t nrhs, int32_t direction, int32_t accumulate,
+                         void *stream);
+
+/* ---- plan API (device pointers, caller stream) -------------------------------------------- */
+
+typedef struct mxb_plan mxb_plan;
+
+/* Host description of a CDS.  Pair lists are flat: near pair k is (npairx[k], npairy[k])
+ * with block D + Dptr[k]; far pair k is (fpairx[k], fpairy[k]) with B + Bptr[k].  For an
+ * HSS CDS set is_hss = 1 and give the far pairs as (i, sibling(i)), i = 1..numnodes-1. */
+typedef struct mxb_cds_desc {
+    int32_t nleaf, numnodes, is_hss;
+    const double *D;   uint64_t D_len;
+    const double *B;   uint64_t B_len;
+    const double *VT;  uint64_t VT_len;
+    const uint64_t *Dptr; const uint64_t *Bptr; const int32_t *VTptr;
+    const int32_t *lchildren, *rchildren, *lm, *slen, *Ddim;
+    const int32_t *npairx, *npairy; int32_t ncount;
+    const int32_t *fpairx, *fpairy; int32_t fcount;
+} mxb_cds_desc;
+
+/* Uploads and repacks the CDS for `precision`, builds the task lists; device = current. */
+MXB_API int32_t mxb_plan_create(const mxb_cds_desc *desc, int32_t precision, mxb_plan **out);
+MXB_API int32_t mxb_plan_destroy(mxb_plan *plan);
+/* dY (+)= K~ dW on `stream` (a cudaStream_t, 0 = legacy default).  dW / dY are device
+ * arrays in the leaf-blocked layout with per-leaf offsets wptr / uptr (host arrays, nleaf
+ * entries; NULL = packed: offset of leaf i = (sum of Ddim[<i]) * nrhs).  accumulate = 1
+ * adds to dY (H2-b reference semantics), 0 overwrites it.  Asynchronous. */
+MXB_API int32_t mxb_plan_evaluate(mxb_plan *plan, const double *dW, double *dY, int32_t nrhs,
+                          const int32_t *wptr, const int32_t *uptr, int32_t accumulate,
+                          void *stream);
+/* dGW (+)= K~^T dG by the transposed traversal (no counterpart in the reference). */
+MXB_API int32_t mxb_plan_adjoint(mxb_plan *plan, const double *dG, double *dGW, int32_t nrhs,
+                         const int32_t *gptr, const int32_t *gwptr, int32_t accumulate,
+                         void *stream);
+/* Algorithmic flops of one evaluation (matroxTest-V1/compression.h:1079-1130). */
+MXB_API int32_t mxb_plan_flops(const mxb_plan *plan, int32_t nrhs, uint64_t *flops);
+/* Bytes of CDS held on the device and number of kernel launches of one evaluation. */
+MXB_API int32_t mxb_plan_info(const mxb_plan *plan, uint64_t *device_bytes, int32_t *launches,
+                      int32_t *precision);
+/* Copies the last evaluation's skeleton workspaces (wskel, uskel) to host arrays laid out
+ * with the caller's wskeloffset / uskeloffset (for callers that inspect them). */
+MXB_API int32_t mxb_plan_read_workspaces(mxb_plan *plan, int32_t nrhs, const int32_t *wskeloffset,
+                                 double *wskel, const int32_t *uskeloffset, double *uskel);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MATROX_B200_H */

@@ -1,0 +1,782 @@
+// C-ABI entry points: the reference-signature drop-ins (host arrays, synchronous) and the
+// device-pointer plan API.
+#include <algorithm>
+#include <cstring>
+#include <list>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "matrox_b200.h"
+#include "mxb_internal.h"
+#include "plan.h"
+
+namespace mxb {
+cudaError_t launch_permute(const int32_t *perm, const int32_t *leafofs, const int32_t *blockofs, int nleaf,
+                           int64_t n, const double *src, double *dst, int64_t rs, int64_t cs, int nrhs,
+                           int dir, int accumulate, cudaStream_t stream);
+}
+
+using namespace mxb;
+
+#define API_CUDA(call)                                                                    \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess) {                                                          \
+            set_error(std::string(#call) + ": " + cudaGetErrorString(e_));                \
+            return MXB_ERR_CUDA;                                                          \
+        }                                                                                 \
+    } while (0)
+
+namespace {
+
+std::mutex g_mu;
+int g_precision = MXB_PREC_FP64;
+uint32_t g_flags = 0;
+int g_shape_nrow = -1, g_shape_frow = -1, g_shape_cdepth = -1;
+int g_hss_nleaf = -1, g_hss_cdepth = -1;
+
+// ---- device copy cache of CDSs seen by the drop-ins ----
+struct CacheEntry {
+    uint64_t key;
+    int device;
+    int precision;
+    std::unique_ptr<Plan> plan;
+};
+std::list<CacheEntry> g_cache;  // most recent first
+constexpr size_t kCacheSlots = 4;
+
+struct DeviceBuffers {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    double *W = nullptr, *Y = nullptr;
+    size_t wcap = 0, ycap = 0;
+};
+DeviceBuffers g_buf[64];
+
+uint64_t fnv(uint64_t h, const void *p, size_t n)
+{
+    const unsigned char *c = static_cast<const unsigned char *>(p);
+    for (size_t i = 0; i < n; ++i) {
+        h ^= c[i];
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+template <class T>
+uint64_t fnv_arr(uint64_t h, const T *p, size_t n)
+{
+    return p ? fnv(h, p, n * sizeof(T)) : fnv(h, "null", 4);
+}
+// sample of a numeric pool: length, first, last and ~4096 evenly spaced values
+uint64_t fnv_sample(uint64_t h, const double *p, uint64_t n)
+{
+    h = fnv(h, &n, sizeof(n));
+    if (!p || !n) return h;
+    const uint64_t step = std::max<uint64_t>(1, n / 4096);
+    for (uint64_t i = 0; i < n; i += step) h = fnv(h, p + i, sizeof(double));
+    return fnv(h, p + n - 1, sizeof(double));
+}
+
+uint64_t desc_key(const mxb_cds_desc &d)
+{
+    uint64_t h = 1469598103934665603ull;
+    const void *ptrs[] = {d.D, d.B, d.VT};
+    h = fnv(h, ptrs, sizeof(ptrs));
+    h = fnv(h, &d.nleaf, sizeof(int32_t) * 3);
+    h = fnv_sample(h, d.D, d.D_len);
+    h = fnv_sample(h, d.B, d.B_len);
+    h = fnv_sample(h, d.VT, d.VT_len);
+    h = fnv_arr(h, d.Dptr, d.ncount);
+    h = fnv_arr(h, d.Bptr, d.fcount);
+    h = fnv_arr(h, d.VTptr, d.numnodes);
+    h = fnv_arr(h, d.lchildren, d.numnodes);
+    h = fnv_arr(h, d.rchildren, d.numnodes);
+    h = fnv_arr(h, d.lm, d.numnodes);
+    h = fnv_arr(h, d.slen, d.numnodes);
+    h = fnv_arr(h, d.Ddim, d.nleaf);
+    h = fnv_arr(h, d.npairx, d.ncount);
+    h = fnv_arr(h, d.npairy, d.ncount);
+    h = fnv_arr(h, d.fpairx, d.fcount);
+    h = fnv_arr(h, d.fpairy, d.fcount);
+    return h;
+}
+
+int cached_plan(const mxb_cds_desc &d, Plan **out)
+{
+    int dev = 0;
+    API_CUDA(cudaGetDevice(&dev));
+    const uint64_t key = desc_key(d);
+    for (auto it = g_cache.begin(); it != g_cache.end(); ++it) {
+        if (it->key == key && it->device == dev && it->precision == g_precision) {
+            g_cache.splice(g_cache.begin(), g_cache, it);
+            *out = g_cache.front().plan.get();
+            return MXB_OK;
+        }
+    }
+    Plan *p = nullptr;
+    int rc = Plan::create(d, g_precision, &p);
+    if (rc) return rc;
+    g_cache.push_front(CacheEntry{key, dev, g_precision, std::unique_ptr<Plan>(p)});
+    while (g_cache.size() > kCacheSlots) g_cache.pop_back();
+    *out = p;
+    return MXB_OK;
+}
+
+DeviceBuffers *buffers()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    DeviceBuffers &b = g_buf[dev];
+    if (!b.stream) {
+        if (cudaStreamCreateWithFlags(&b.stream, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+        b.device = dev;
+    }
+    return &b;
+}
+
+int grow(double **p, size_t *cap, size_t elems)
+{
+    if (elems <= *cap) return MXB_OK;
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    cudaError_t e = cudaMalloc(p, std::max<size_t>(elems, 1) * sizeof(double));
+    if (e != cudaSuccess) {
+        set_error(std::string("cudaMalloc for drop-in operands: ") + cudaGetErrorString(e));
+        return e == cudaErrorMemoryAllocation ? MXB_ERR_NOMEM : MXB_ERR_CUDA;
+    }
+    *cap = elems;
+    return MXB_OK;
+}
+
+// Flat pair list from the reference's CSR-of-CSR blocking (nblockSet -> nblocks -> pairs);
+// the pair index k addresses Dptr / Bptr directly, as in codeGen/H2GEMM.h:395-404.
+int flatten_blocked(const int32_t *set, const int32_t *blocks, int nrow, std::vector<int> &ks)
+{
+    ks.clear();
+    if (nrow < 0) {
+        set_error("negative block-row count");
+        return MXB_ERR_ARG;
+    }
+    if (nrow == 0) return MXB_OK;
+    if (!set || !blocks) {
+        set_error("null blocking array");
+        return MXB_ERR_ARG;
+    }
+    for (int i = 0; i < nrow; ++i) {
+        if (set[i] > set[i + 1] || set[i] < 0) {
+            set_error("blockset not monotone");
+            return MXB_ERR_STRUCTURE;
+        }
+        for (int j = set[i]; j < set[i + 1]; ++j) {
+            if (blocks[j] > blocks[j + 1] || blocks[j] < 0) {
+                set_error("blocks not monotone");
+                return MXB_ERR_STRUCTURE;
+            }
+            for (int k = blocks[j]; k < blocks[j + 1]; ++k) ks.push_back(k);
+        }
+    }
+    return MXB_OK;
+}
+
+struct DropIn {
+    // reference arrays
+    double *D, *B, *VT;
+    uint64_t *Dptr, *Bptr;
+    int32_t *VTptr, *lch, *rch, *Ddim, *wptr, *uptr, *wsko, *usko, *lm, *slen;
+    double *mrhs, *apres, *wskel, *uskel;
+    int32_t nrhs;
+    int nleaf, numnodes;
+    bool hss;
+    std::vector<int32_t> px, py, fx, fy;
+    std::vector<uint64_t> dofs, bofs;
+};
+
+int run_dropin(DropIn &a)
+{
+    if (!a.D || !a.VT || !a.Dptr || !a.VTptr || !a.lch || !a.rch || !a.Ddim || !a.wptr || !a.uptr || !a.lm ||
+        !a.slen || !a.mrhs || !a.apres) {
+        set_error("null argument");
+        return MXB_ERR_ARG;
+    }
+    if (a.nrhs < 1 || a.nleaf < 1 || a.numnodes < 1) {
+        set_error("nrhs, nleaf and numnodes must be >= 1");
+        return MXB_ERR_ARG;
+    }
+    // array extents implied by the offsets (the reference passes none)
+    uint64_t D_len = 0, B_len = 0, VT_len = 0;
+    for (size_t k = 0; k < a.px.size(); ++k) {
+        const int x = a.px[k], y = a.py[k];
+        if (x < 0 || x >= a.nleaf || y < 0 || y >= a.nleaf) {
+            set_error("near pair index out of range");
+            return MXB_ERR_STRUCTURE;
+        }
+        D_len = std::max<uint64_t>(D_len, a.dofs[k] + (uint64_t)a.Ddim[x] * a.Ddim[y]);
+    }
+    for (size_t k = 0; k < a.fx.size(); ++k) {
+        const int x = a.fx[k], y = a.fy[k];
+        if (x < 0 || x >= a.numnodes || y < 0 || y >= a.numnodes) {
+            set_error("far pair index out of range");
+            return MXB_ERR_STRUCTURE;
+        }
+        B_len = std::max<uint64_t>(B_len, a.bofs[k] + (uint64_t)a.slen[x] * a.slen[y]);
+    }
+    for (int v = 0; v < a.numnodes; ++v) {
+        if (a.slen[v] <= 0) continue;
+        const int l = a.lch[v], r = a.rch[v];
+        uint64_t cols;
+        if (l == -1) {
+            if (a.lm[v] < 0 || a.lm[v] >= a.nleaf) {
+                set_error("leaf map out of range");
+                return MXB_ERR_STRUCTURE;
+            }
+            cols = (uint64_t)a.Ddim[a.lm[v]];
+        } else {
+            if (l < 0 || l >= a.numnodes || r < 0 || r >= a.numnodes) {
+                set_error("child index out of range");
+                return MXB_ERR_STRUCTURE;
+            }
+            cols = (uint64_t)a.slen[l] + a.slen[r];
+        }
+        if (a.VTptr[v] < 0) {
+            set_error("negative VTptr");
+            return MXB_ERR_STRUCTURE;
+        }
+        VT_len = std::max<uint64_t>(VT_len, (uint64_t)a.VTptr[v] + (uint64_t)a.slen[v] * cols);
+    }
+    if (!a.fx.empty() && !a.B) {
+        set_error("null B with far pairs");
+        return MXB_ERR_ARG;
+    }
+    mxb_cds_desc d{};
+    d.nleaf = a.nleaf;
+    d.numnodes = a.numnodes;
+    d.is_hss = a.hss;
+    d.D = a.D;
+    d.D_len = D_len;
+    d.B = a.B;
+    d.B_len = B_len;
+    d.VT = a.VT;
+    d.VT_len = VT_len;
+    d.Dptr = a.dofs.data();
+    d.Bptr = a.bofs.data();
+    d.VTptr = a.VTptr;
+    d.lchildren = a.lch;
+    d.rchildren = a.rch;
+    d.lm = a.lm;
+    d.slen = a.slen;
+    d.Ddim = a.Ddim;
+    d.npairx = a.px.data();
+    d.npairy = a.py.data();
+    d.ncount = (int32_t)a.px.size();
+    d.fpairx = a.fx.data();
+    d.fpairy = a.fy.data();
+    d.fcount = (int32_t)a.fx.size();
+
+    std::lock_guard<std::mutex> lock(g_mu);
+    Plan *plan = nullptr;
+    int rc = cached_plan(d, &plan);
+    if (rc) return rc;
+    DeviceBuffers *buf = buffers();
+    if (!buf) {
+        set_error("cannot create the drop-in stream");
+        return MXB_ERR_CUDA;
+    }
+    // extents of the caller's leaf-blocked W and Y
+    size_t wext = 0, yext = 0;
+    for (int i = 0; i < a.nleaf; ++i) {
+        if (a.wptr[i] < 0 || a.uptr[i] < 0) {
+            set_error("negative leaf offset");
+            return MXB_ERR_STRUCTURE;
+        }
+        wext = std::max<size_t>(wext, (size_t)a.wptr[i] + (size_t)a.Ddim[i] * a.nrhs);
+        yext = std::max<size_t>(yext, (size_t)a.uptr[i] + (size_t)a.Ddim[i] * a.nrhs);
+    }
+    rc = grow(&buf->W, &buf->wcap, wext);
+    if (rc) return rc;
+    rc = grow(&buf->Y, &buf->ycap, yext);
+    if (rc) return rc;
+    cudaStream_t s = buf->stream;
+    API_CUDA(cudaMemcpyAsync(buf->W, a.mrhs, wext * sizeof(double), cudaMemcpyHostToDevice, s));
+    const bool accumulate = !a.hss;
+    if (accumulate && !(g_flags & MXB_FLAG_OUTPUT_IS_ZERO))
+        API_CUDA(cudaMemcpyAsync(buf->Y, a.apres, yext * sizeof(double), cudaMemcpyHostToDevice, s));
+    else if (accumulate)
+        API_CUDA(cudaMemsetAsync(buf->Y, 0, yext * sizeof(double), s));
+    rc = plan->run(plan->launches_fwd, buf->W, buf->Y, a.nrhs, a.wptr, a.uptr, accumulate ? 1 : 0, s);
+    if (rc) return rc;
+    API_CUDA(cudaMemcpyAsync(a.apres, buf->Y, yext * sizeof(double), cudaMemcpyDeviceToHost, s));
+    API_CUDA(cudaStreamSynchronize(s));
+    if ((g_flags & MXB_FLAG_MIRROR_WORKSPACES) && plan->precision == MXB_PREC_FP64) {
+        rc = plan->read_workspaces(a.nrhs, a.wsko, a.wskel, a.usko, a.uskel);
+        if (rc) return rc;
+    }
+    return MXB_OK;
+}
+
+void fill_common(DropIn &a, double *D, double *B, double *VT, uint64_t *Dptr, uint64_t *Bptr, int32_t *VTptr,
+                 int32_t *lchildren, int32_t *rchildren, double *mrhs, double *apres, int32_t nrhs,
+                 int32_t *Ddim, int32_t *wptr, int32_t *uptr, double *wskel, int32_t *wskeloffset, double *uskel,
+                 int32_t *uskeloffset, int32_t *lm, int32_t *slen)
+{
+    a.D = D;
+    a.B = B;
+    a.VT = VT;
+    a.Dptr = Dptr;
+    a.Bptr = Bptr;
+    a.VTptr = VTptr;
+    a.lch = lchildren;
+    a.rch = rchildren;
+    a.mrhs = mrhs;
+    a.apres = apres;
+    a.nrhs = nrhs;
+    a.Ddim = Ddim;
+    a.wptr = wptr;
+    a.uptr = uptr;
+    a.wskel = wskel;
+    a.wsko = wskeloffset;
+    a.uskel = uskel;
+    a.usko = uskeloffset;
+    a.lm = lm;
+    a.slen = slen;
+}
+
+// numnodes from a schedule: the coarsened (or plain) level sets list every node but the
+// root once, so numnodes = entries + 1 and nleaf = (numnodes + 1) / 2 for a full binary tree.
+int sizes_from_schedule(int entries, DropIn &a)
+{
+    if (entries < 0) {
+        set_error("schedule arrays are inconsistent");
+        return MXB_ERR_STRUCTURE;
+    }
+    a.numnodes = entries + 1;
+    a.nleaf = (a.numnodes + 1) / 2;
+    return MXB_OK;
+}
+
+int h2b_common(DropIn &a, int32_t *nblockSet, int32_t *nblocks, int32_t *npairx, int32_t *npairy,
+               int32_t *fblockSet, int32_t *fblocks, int32_t *fpairx, int32_t *fpairy, int nrow, int frow)
+{
+    std::vector<int> ks;
+    int rc = flatten_blocked(nblockSet, nblocks, nrow, ks);
+    if (rc) return rc;
+    if (!ks.empty() && (!npairx || !npairy)) {
+        set_error("null near pair arrays");
+        return MXB_ERR_ARG;
+    }
+    a.hss = false;
+    for (int k : ks) {
+        a.px.push_back(npairx[k]);
+        a.py.push_back(npairy[k]);
+        a.dofs.push_back(a.Dptr[k]);
+    }
+    rc = flatten_blocked(fblockSet, fblocks, frow, ks);
+    if (rc) return rc;
+    if (!ks.empty() && (!fpairx || !fpairy || !a.Bptr)) {
+        set_error("null far pair arrays");
+        return MXB_ERR_ARG;
+    }
+    for (int k : ks) {
+        a.fx.push_back(fpairx[k]);
+        a.fy.push_back(fpairy[k]);
+        a.bofs.push_back(a.Bptr[k]);
+    }
+    return run_dropin(a);
+}
+
+int hss_common(DropIn &a, int ncount, int fcount)
+{
+    a.hss = true;
+    if (ncount != a.nleaf || fcount != a.numnodes - 1) {
+        set_error("HSS ncount / fcount do not match the level sets (ncount = leaves, fcount = numnodes - 1)");
+        return MXB_ERR_STRUCTURE;
+    }
+    for (int i = 0; i < ncount; ++i) {
+        a.px.push_back(i);
+        a.py.push_back(i);
+        a.dofs.push_back(a.Dptr[i]);
+    }
+    if (fcount > 0 && !a.Bptr) {
+        set_error("null Bptr");
+        return MXB_ERR_ARG;
+    }
+    for (int i = 1; i < fcount + 1; ++i) {
+        a.fx.push_back(i);
+        a.fy.push_back((i & 1) == 0 ? i - 1 : i + 1);
+        a.bofs.push_back(a.Bptr[i - 1]);
+    }
+    return run_dropin(a);
+}
+
+int coarse_entries(const int32_t *wpart, const int32_t *clevelset, int cdepth)
+{
+    if (!wpart || !clevelset || cdepth < 0) return -1;
+    return wpart[clevelset[cdepth]] - wpart[clevelset[0]];
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *mxb_last_error(void) { return mxb::last_error(); }
+const char *mxb_version(void) { return "matrox_b200 0.1 (sm_100a)"; }
+
+int32_t mxb_set_precision(int32_t mode)
+{
+    if (mode != MXB_PREC_FP64 && mode != MXB_PREC_SPLIT_BF16) {
+        set_error("unknown precision mode");
+        return MXB_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lock(g_mu);
+    g_precision = mode;
+    return MXB_OK;
+}
+
+int32_t mxb_set_flags(uint32_t flags)
+{
+    std::lock_guard<std::mutex> lock(g_mu);
+    g_flags = flags;
+    return MXB_OK;
+}
+
+int32_t mxb_cache_invalidate(void)
+{
+    std::lock_guard<std::mutex> lock(g_mu);
+    g_cache.clear();
+    return MXB_OK;
+}
+
+int32_t CBHGEMM(double *D, double *B, double *VT, uint64_t *Dptr, uint64_t *Bptr, int32_t *VTptr,
+                int32_t *lchildren, int32_t *rchildren, int32_t *levelset, int32_t *idx, double *mrhs,
+                double *apres, int32_t nrhs, int32_t *Ddim, int32_t *wptr, int32_t *uptr, double *wskel,
+                int32_t *wskeloffset, double *uskel, int32_t *uskeloffset, int32_t *lm, int32_t *slen,
+                int32_t *nblockSet, int32_t *nblocks, int32_t *npairx, int32_t *npairy, int32_t *fblockSet,
+                int32_t *fblocks, int32_t *fpairx, int32_t *fpairy, int32_t ncount, int32_t fcount,
+                int32_t *wpart, int32_t *clevelset, int cdepth)
+{
+    (void)levelset;
+    (void)idx;
+    DropIn a{};
+    fill_common(a, D, B, VT, Dptr, Bptr, VTptr, lchildren, rchildren, mrhs, apres, nrhs, Ddim, wptr, uptr, wskel,
+                wskeloffset, uskel, uskeloffset, lm, slen);
+    int rc = sizes_from_schedule(coarse_entries(wpart, clevelset, cdepth), a);
+    if (rc) return rc;
+    return h2b_common(a, nblockSet, nblocks, npairx, npairy, fblockSet, fblocks, fpairx, fpairy, ncount, fcount);
+}
+
+int32_t lowH2GEMM(double *D, double *B, double *VT, uint64_t *Dptr, uint64_t *Bptr, int32_t *VTptr,
+                  int32_t *lchildren, int32_t *rchildren, int32_t *levelset, int32_t *idx, double *mrhs,
+                  double *apres, int32_t nrhs, int32_t *Ddim, int32_t *wptr, int32_t *uptr, double *wskel,
+                  int32_t *wskeloffset, double *uskel, int32_t *uskeloffset, int32_t *lm, int32_t *slen,
+                  int32_t *nblockSet, int32_t *nblocks, int32_t *npairx, int32_t *npairy, int32_t *fblockSet,
+                  int32_t *fblocks, int32_t *fpairx, int32_t *fpairy, int32_t ncount, int32_t fcount,
+                  int32_t *wpart, int32_t *clevelset, int cdepth)
+{
+    return CBHGEMM(D, B, VT, Dptr, Bptr, VTptr, lchildren, rchildren, levelset, idx, mrhs, apres, nrhs, Ddim, wptr,
+                   uptr, wskel, wskeloffset, uskel, uskeloffset, lm, slen, nblockSet, nblocks, npairx, npairy,
+                   fblockSet, fblocks, fpairx, fpairy, ncount, fcount, wpart, clevelset, cdepth);
+}
+
+int32_t blockGEMM(double *D, double *B, double *VT, uint64_t *Dptr, uint64_t *Bptr, int32_t *VTptr,
+                  int32_t *lchildren, int32_t *rchildren, int32_t *levelset, int32_t *idx, double *mrhs,
+                  double *apres, int32_t nrhs, int32_t *Ddim, int32_t *wptr, int32_t *uptr, double *wskel,
+                  int32_t *wskeloffset, double *uskel, int32_t *uskeloffset, int32_t *lm, int32_t *slen,
+                  int32_t *nblockSet, int32_t *nblocks, int32_t *npairx, int32_t *npairy, int32_t *fblockSet,
+                  int32_t *fblocks, int32_t *fpairx, int32_t *fpairy, int32_t ncount, int32_t fcount,
+                  int32_t depth)
+{
+    (void)idx;
+    DropIn a{};
+    fill_common(a, D, B, VT, Dptr, Bptr, VTptr, lchildren, rchildren, mrhs, apres, nrhs, Ddim, wptr, uptr, wskel,
+                wskeloffset, uskel, uskeloffset, lm, slen);
+    if (!levelset || depth < 0) {
+        set_error("null levelset");
+        return MXB_ERR_ARG;
+    }
+    int rc = sizes_from_schedule(levelset[depth] - levelset[0], a);
+    if (rc) return rc;
+    return h2b_common(a, nblockSet, nblocks, npairx, npairy, fblockSet, fblocks, fpairx, fpairy, ncount, fcount);
+}
+
+int32_t mxb_hgemm_set_shape(int32_t nrow, int32_t frow, int32_t cdepth)
+{
+    if (nrow < 0 || frow < 0 || cdepth < 0) {
+        set_error("negative shape");
+        return MXB_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lock(g_mu);
+    g_shape_nrow = nrow;
+    g_shape_frow = frow;
+    g_shape_cdepth = cdepth;
+    return MXB_OK;
+}
+
+int32_t HGEMM(double *D, double *B, double *VT, uint64_t *Dptr, uint64_t *Bptr, int32_t *VTptr,
+              int32_t *lchildren, int32_t *rchildren, int32_t *levelset, int32_t *idx, double *mrhs,
+              double *apres, int32_t nrhs, int32_t *Ddim, int32_t *wptr, int32_t *uptr, double *wskel,
+              int32_t *wskeloffset, double *uskel, int32_t *uskeloffset, int32_t *lm, int32_t *slen,
+              int32_t *nblockSet, int32_t *nblocks, int32_t *npairx, int32_t *npairy, int32_t *fblockSet,
+              int32_t *fblocks, int32_t *fpairx, int32_t *fpairy, int32_t *wpart, int32_t *clevelset)
+{
+    int nrow, frow, cdepth;
+    {
+        std::lock_guard<std::mutex> lock(g_mu);
+        nrow = g_shape_nrow;
+        frow = g_shape_frow;
+        cdepth = g_shape_cdepth;
+    }
+    if (nrow < 0) {
+        set_error("HGEMM: call mxb_hgemm_set_shape first (the generated code bakes these sizes in)");
+        return MXB_ERR_ARG;
+    }
+    return CBHGEMM(D, B, VT, Dptr, Bptr, VTptr, lchildren, rchildren, levelset, idx, mrhs, apres, nrhs, Ddim, wptr,
+                   uptr, wskel, wskeloffset, uskel, uskeloffset, lm, slen, nblockSet, nblocks, npairx, npairy,
+                   fblockSet, fblocks, fpairx, fpairy, nrow, frow, wpart, clevelset, cdepth);
+}
+
+int32_t parHSSGEMM(double *D, double *B, double *VT, uint64_t *Dptr, uint64_t *Bptr, int32_t *VTptr,
+                   int32_t *lchildren, int32_t *rchildren, int32_t *levelset, int32_t *idx, double *mrhs,
+                   double *apres, int32_t nrhs, int32_t *Ddim, int32_t *wptr, int32_t *uptr, double *wskel,
+                   int32_t *wskeloffset, double *uskel, int32_t *uskeloffset, int32_t *lm, int32_t *slen,
+                   int32_t *wpart, int32_t *clevelset, int ncount, int fcount, int cdepth)
+{
+    (void)levelset;
+    (void)idx;
+    DropIn a{};
+    fill_common(a, D, B, VT, Dptr, Bptr, VTptr, lchildren, rchildren, mrhs, apres, nrhs, Ddim, wptr, uptr, wskel,
+                wskeloffset, uskel, uskeloffset, lm, slen);
+    int rc = sizes_from_schedule(coarse_entries(wpart, clevelset, cdepth), a);
+    if (rc) return rc;
+    return hss_common(a, ncount, fcount);
+}
+
+int32_t lowHSSGEMM(double *D, double *B, double *VT, uint64_t *Dptr, uint64_t *Bptr, int32_t *VTptr,
+                   int32_t *lchildren, int32_t *rchildren, int32_t *levelset, int32_t *idx, double *mrhs,
+                   double *apres, int32_t nrhs, int32_t *Ddim, int32_t *wptr, int32_t *uptr, double *wskel,
+                   int32_t *wskeloffset, double *uskel, int32_t *uskeloffset, int32_t *lm, int32_t *slen,
+                   int32_t *wpart, int32_t *clevelset, int ncount, int fcount, int cdepth)
+{
+    return parHSSGEMM(D, B, VT, Dptr, Bptr, VTptr, lchildren, rchildren, levelset, idx, mrhs, apres, nrhs, Ddim,
+                      wptr, uptr, wskel, wskeloffset, uskel, uskeloffset, lm, slen, wpart, clevelset, ncount, fcount,
+                      cdepth);
+}
+
+int32_t seqHSSGEMM(double *D, double *B, double *VT, uint64_t *Dptr, uint64_t *Bptr, int32_t *VTptr,
+                   int32_t *lchildren, int32_t *rchildren, int32_t *levelset, int32_t *idx, double *mrhs,
+                   double *apres, int32_t nrhs, int32_t *Ddim, int32_t *wptr, int32_t *uptr, double *wskel,
+                   int32_t *wskeloffset, double *uskel, int32_t *uskeloffset, int32_t *lm, int32_t *slen,
+                   int32_t ncount, int32_t fcount, int32_t depth)
+{
+    (void)idx;
+    DropIn a{};
+    fill_common(a, D, B, VT, Dptr, Bptr, VTptr, lchildren, rchildren, mrhs, apres, nrhs, Ddim, wptr, uptr, wskel,
+                wskeloffset, uskel, uskeloffset, lm, slen);
+    if (!levelset || depth < 0) {
+        set_error("null levelset");
+        return MXB_ERR_ARG;
+    }
+    int rc = sizes_from_schedule(levelset[depth] - levelset[0], a);
+    if (rc) return rc;
+    return hss_common(a, ncount, fcount);
+}
+
+int32_t mxb_hgemm_hss_set_shape(int32_t nleaf, int32_t cdepth)
+{
+    if (nleaf < 1 || cdepth < 0) {
+        set_error("bad HSS shape");
+        return MXB_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lock(g_mu);
+    g_hss_nleaf = nleaf;
+    g_hss_cdepth = cdepth;
+    return MXB_OK;
+}
+
+int32_t HGEMM_HSS(double *D, double *B, double *VT, uint64_t *Dptr, uint64_t *Bptr, int32_t *VTptr,
+                  int32_t *lchildren, int32_t *rchildren, int32_t *levelset, int32_t *idx, double *mrhs,
+                  double *apres, int32_t nrhs, int32_t *Ddim, int32_t *wptr, int32_t *uptr, double *wskel,
+                  int32_t *wskeloffset, double *uskel, int32_t *uskeloffset, int32_t *lm, int32_t *slen,
+                  int32_t *wpart, int32_t *clevelset)
+{
+    int nleaf, cdepth;
+    {
+        std::lock_guard<std::mutex> lock(g_mu);
+        nleaf = g_hss_nleaf;
+        cdepth = g_hss_cdepth;
+    }
+    if (nleaf < 1) {
+        set_error("HGEMM_HSS: call mxb_hgemm_hss_set_shape first");
+        return MXB_ERR_ARG;
+    }
+    return parHSSGEMM(D, B, VT, Dptr, Bptr, VTptr, lchildren, rchildren, levelset, idx, mrhs, apres, nrhs, Ddim,
+                      wptr, uptr, wskel, wskeloffset, uskel, uskeloffset, lm, slen, wpart, clevelset, nleaf,
+                      2 * nleaf - 2, cdepth);
+}
+
+// ---- permutation -----------------------------------------------------------------------
+
+int32_t mxb_permute_rows(const int32_t *d_perm, const int32_t *d_leafofs, const int32_t *d_blockofs,
+                         int32_t nleaf, int64_t n, const double *src, double *dst, int64_t row_stride,
+                         int64_t col_stride, int32_t nrhs, int32_t direction, int32_t accumulate, void *stream)
+{
+    if (!d_perm || !d_leafofs || !d_blockofs || !src || !dst || nleaf < 1 || n < 0 || nrhs < 0 ||
+        (direction != 0 && direction != 1)) {
+        set_error("mxb_permute_rows: bad argument");
+        return MXB_ERR_ARG;
+    }
+    API_CUDA(launch_permute(d_perm, d_leafofs, d_blockofs, nleaf, n, src, dst, row_stride, col_stride, nrhs,
+                            direction, accumulate, (cudaStream_t)stream));
+    return MXB_OK;
+}
+
+static int host_permute(const int32_t *perm, const int32_t *leafofs, const int32_t *blockofs, int32_t nleaf,
+                        const double *src, int64_t n, int64_t ld, int32_t nrhs, double *dst, int dir)
+{
+    if (!perm || !leafofs || !blockofs || !src || !dst || nleaf < 1 || n < 0 || nrhs < 1 || ld < n) {
+        set_error("transform: bad argument");
+        return MXB_ERR_ARG;
+    }
+    if (leafofs[0] != 0 || leafofs[nleaf] != n) {
+        set_error("transform: leaf offsets must cover [0, n)");
+        return MXB_ERR_STRUCTURE;
+    }
+    size_t blk_ext = 0;
+    for (int i = 0; i < nleaf; ++i)
+        blk_ext = std::max<size_t>(blk_ext, (size_t)blockofs[i] + (size_t)(leafofs[i + 1] - leafofs[i]) * nrhs);
+    for (int64_t t = 0; t < n; ++t)
+        if (perm[t] < 0 || perm[t] >= n) {
+            set_error("transform: permutation entry out of range");
+            return MXB_ERR_STRUCTURE;
+        }
+    std::lock_guard<std::mutex> lock(g_mu);
+    DeviceBuffers *buf = buffers();
+    if (!buf) return MXB_ERR_CUDA;
+    cudaStream_t s = buf->stream;
+    const size_t mat = (size_t)ld * nrhs;
+    int32_t *di = nullptr;
+    double *dm = nullptr, *db = nullptr;
+    const size_t ni = (size_t)n + 2 * ((size_t)nleaf + 1);
+    API_CUDA(cudaMalloc(&di, ni * sizeof(int32_t)));
+    cudaError_t e = cudaMalloc(&dm, mat * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&db, std::max<size_t>(blk_ext, 1) * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(di, perm, n * sizeof(int32_t), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(di + n, leafofs, (nleaf + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(di + n + nleaf + 1, blockofs, nleaf * sizeof(int32_t), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) {
+        if (dir == 0) {
+            e = cudaMemcpyAsync(dm, src, mat * sizeof(double), cudaMemcpyHostToDevice, s);
+            if (e == cudaSuccess)
+                e = launch_permute(di, di + n, di + n + nleaf + 1, nleaf, n, dm, db, 1, ld, nrhs, 0, 0, s);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(dst, db, blk_ext * sizeof(double), cudaMemcpyDeviceToHost, s);
+        } else {
+            e = cudaMemcpyAsync(db, src, blk_ext * sizeof(double), cudaMemcpyHostToDevice, s);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(dm, dst, mat * sizeof(double), cudaMemcpyHostToDevice, s);
+            if (e == cudaSuccess)
+                e = launch_permute(di, di + n, di + n + nleaf + 1, nleaf, n, db, dm, 1, ld, nrhs, 1, 0, s);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(dst, dm, mat * sizeof(double), cudaMemcpyDeviceToHost, s);
+        }
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(di);
+    cudaFree(dm);
+    cudaFree(db);
+    if (e != cudaSuccess) {
+        set_error(std::string("transform: ") + cudaGetErrorString(e));
+        return MXB_ERR_CUDA;
+    }
+    return MXB_OK;
+}
+
+int32_t mxb_transform(const int32_t *perm, const int32_t *leafofs, const int32_t *wptr, int32_t nleaf,
+                      const double *W, int64_t n, int64_t ldw, int32_t nrhs, double *TW)
+{
+    return host_permute(perm, leafofs, wptr, nleaf, W, n, ldw, nrhs, TW, 0);
+}
+
+int32_t mxb_untransform(const int32_t *perm, const int32_t *leafofs, const int32_t *uptr, int32_t nleaf,
+                        const double *TY, int64_t n, int64_t ldy, int32_t nrhs, double *Y)
+{
+    return host_permute(perm, leafofs, uptr, nleaf, TY, n, ldy, nrhs, Y, 1);
+}
+
+// ---- plan API ------------------------------------------------------------------------------
+
+int32_t mxb_plan_create(const mxb_cds_desc *desc, int32_t precision, mxb_plan **out)
+{
+    if (!desc || !out) {
+        set_error("null argument");
+        return MXB_ERR_ARG;
+    }
+    Plan *p = nullptr;
+    int rc = Plan::create(*desc, precision, &p);
+    if (rc) return rc;
+    *out = p;
+    return MXB_OK;
+}
+
+int32_t mxb_plan_destroy(mxb_plan *plan)
+{
+    delete static_cast<Plan *>(plan);
+    return MXB_OK;
+}
+
+int32_t mxb_plan_evaluate(mxb_plan *plan, const double *dW, double *dY, int32_t nrhs, const int32_t *wptr,
+                          const int32_t *uptr, int32_t accumulate, void *stream)
+{
+    if (!plan) {
+        set_error("null plan");
+        return MXB_ERR_ARG;
+    }
+    Plan *p = static_cast<Plan *>(plan);
+    return p->run(p->launches_fwd, dW, dY, nrhs, wptr, uptr, accumulate, (cudaStream_t)stream);
+}
+
+int32_t mxb_plan_adjoint(mxb_plan *plan, const double *dG, double *dGW, int32_t nrhs, const int32_t *gptr,
+                         const int32_t *gwptr, int32_t accumulate, void *stream)
+{
+    if (!plan) {
+        set_error("null plan");
+        return MXB_ERR_ARG;
+    }
+    Plan *p = static_cast<Plan *>(plan);
+    return p->run(p->launches_adj, dG, dGW, nrhs, gptr, gwptr, accumulate, (cudaStream_t)stream);
+}
+
+int32_t mxb_plan_flops(const mxb_plan *plan, int32_t nrhs, uint64_t *flops)
+{
+    if (!plan || !flops || nrhs < 0) {
+        set_error("bad argument");
+        return MXB_ERR_ARG;
+    }
+    *flops = static_cast<const Plan *>(plan)->flops(nrhs);
+    return MXB_OK;
+}
+
+int32_t mxb_plan_info(const mxb_plan *plan, uint64_t *device_bytes, int32_t *launches, int32_t *precision)
+{
+    if (!plan) {
+        set_error("null plan");
+        return MXB_ERR_ARG;
+    }
+    const Plan *p = static_cast<const Plan *>(plan);
+    if (device_bytes) *device_bytes = p->device_bytes;
+    if (launches) *launches = (int32_t)p->launches_fwd.size();
+    if (precision) *precision = p->precision;
+    return MXB_OK;
+}
+
+int32_t mxb_plan_read_workspaces(mxb_plan *plan, int32_t nrhs, const int32_t *wskeloffset, double *wskel,
+                                 const int32_t *uskeloffset, double *uskel)
+{
+    if (!plan) {
+        set_error("null plan");
+        return MXB_ERR_ARG;
+    }
+    return static_cast<Plan *>(plan)->read_workspaces(nrhs, wskeloffset, wskel, uskeloffset, uskel);
+}
+
+}  // extern "C"

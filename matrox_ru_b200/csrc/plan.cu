@@ -1,0 +1,520 @@
+// Plan: validated structure, device copy of the CDS and the task lists of every pass.
+//
+// Schedule of one evaluation (the reference runs the same four phases,
+// symGen/HGEMM_gen.h:125-236, but as thousands of separate DGEMM calls):
+//   1. leaf up        wskel[v] = P_v W[leaf v]                          (one launch)
+//   2. transfer up    wskel[v] = P_v [wskel[l]; wskel[r]]    one launch per height, bottom-up
+//   3. far + down     uskel[c] = sum_y B_cy wskel[y] + P_p[:, c]^T uskel[p]
+//                                                            one launch per depth, top-down
+//   4. near + leaf down  Y[x] (+)= sum_y D_xy W[y] + P_x^T uskel[x]        (one launch)
+// Phase 3 fuses the far coupling with the downward transfer and phase 4 fuses the near
+// field with the leaf projection, so each skeleton block and each Y block is written
+// exactly once per evaluation.  The adjoint reuses phases 1-2 on G and runs phases 3-4
+// with every near block and far coupling transposed.
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "matrox_b200.h"
+#include "mxb_internal.h"
+#include "plan.h"
+
+namespace mxb {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+const char *last_error() { return g_last_error.c_str(); }
+
+#define MXB_CUDA(call)                                                                    \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess) {                                                          \
+            set_error(std::string(#call) + ": " + cudaGetErrorString(e_));                \
+            return MXB_ERR_CUDA;                                                          \
+        }                                                                                 \
+    } while (0)
+
+int row_tile_for(int precision);
+
+Plan::~Plan()
+{
+    for (void *p : allocations) cudaFree(p);
+}
+
+int Plan::alloc(void **p, size_t bytes)
+{
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        set_error(std::string("cudaMalloc(") + std::to_string(bytes) + "): " + cudaGetErrorString(e));
+        return e == cudaErrorMemoryAllocation ? MXB_ERR_NOMEM : MXB_ERR_CUDA;
+    }
+    allocations.push_back(*p);
+    device_bytes += bytes;
+    return MXB_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// validation of the host structure
+// ---------------------------------------------------------------------------------------
+
+static int fail(const std::string &m)
+{
+    set_error(m);
+    return MXB_ERR_STRUCTURE;
+}
+
+int Plan::validate(const mxb_cds_desc &d)
+{
+    if (d.nleaf < 1 || d.numnodes < 1 || d.ncount < 0 || d.fcount < 0) {
+        set_error("nleaf, numnodes must be >= 1 and pair counts >= 0");
+        return MXB_ERR_ARG;
+    }
+    if (!d.D || !d.Dptr || !d.lchildren || !d.rchildren || !d.lm || !d.slen || !d.Ddim ||
+        (d.ncount && (!d.npairx || !d.npairy)) || (d.fcount && (!d.fpairx || !d.fpairy || !d.B || !d.Bptr)) ||
+        (d.numnodes > 1 && (!d.VT || !d.VTptr))) {
+        set_error("null array in CDS description");
+        return MXB_ERR_ARG;
+    }
+    nleaf = d.nleaf;
+    numnodes = d.numnodes;
+    is_hss = d.is_hss;
+    Ddim.assign(d.Ddim, d.Ddim + nleaf);
+    slen.assign(d.slen, d.slen + numnodes);
+    lch.assign(d.lchildren, d.lchildren + numnodes);
+    rch.assign(d.rchildren, d.rchildren + numnodes);
+    lm.assign(d.lm, d.lm + numnodes);
+    parent.assign(numnodes, -1);
+    for (int i = 0; i < nleaf; ++i)
+        if (Ddim[i] < 1) return fail("Ddim[" + std::to_string(i) + "] < 1");
+    std::vector<int> leafseen(nleaf, 0);
+    for (int v = 0; v < numnodes; ++v) {
+        if (slen[v] < 0) return fail("negative rank at node " + std::to_string(v));
+        const int l = lch[v], r = rch[v];
+        if ((l == -1) != (r == -1)) return fail("node " + std::to_string(v) + " has one child");
+        if (l == -1) {
+            if (lm[v] < 0 || lm[v] >= nleaf) return fail("leaf " + std::to_string(v) + " has no leaf index");
+            if (leafseen[lm[v]]++) return fail("leaf index used twice");
+        } else {
+            if (l < 0 || l >= numnodes || r < 0 || r >= numnodes || l == r || l == v || r == v)
+                return fail("child index out of range at node " + std::to_string(v));
+            if (parent[l] != -1 || parent[r] != -1) return fail("node with two parents");
+            parent[l] = v;
+            parent[r] = v;
+        }
+    }
+    for (int i = 0; i < nleaf; ++i)
+        if (!leafseen[i]) return fail("leaf index " + std::to_string(i) + " unused");
+    root = -1;
+    for (int v = 0; v < numnodes; ++v)
+        if (parent[v] == -1) {
+            if (root != -1) return fail("more than one root");
+            root = v;
+        }
+    if (root == -1) return fail("no root");
+    // depth (from root) and height (from leaves); detects cycles by counting visits
+    depth.assign(numnodes, -1);
+    height.assign(numnodes, 0);
+    std::vector<int> order;
+    order.reserve(numnodes);
+    order.push_back(root);
+    depth[root] = 0;
+    for (size_t i = 0; i < order.size(); ++i) {
+        const int v = order[i];
+        if (lch[v] != -1) {
+            for (int c : {lch[v], rch[v]}) {
+                if (depth[c] != -1) return fail("cycle in tree");
+                depth[c] = depth[v] + 1;
+                order.push_back(c);
+            }
+        }
+    }
+    if ((int)order.size() != numnodes) return fail("tree does not span all nodes");
+    for (int i = numnodes - 1; i >= 0; --i) {
+        const int v = order[i];
+        if (lch[v] != -1) height[v] = 1 + std::max(height[lch[v]], height[rch[v]]);
+    }
+    bfs = order;
+
+    // ranks of leaves may not exceed their sizes' usefulness but any s >= 0 is allowed;
+    // check projection extents
+    VT_len = d.VT_len;
+    for (int v = 0; v < numnodes; ++v) {
+        if (v == root || slen[v] == 0) continue;
+        const uint64_t cols = (lch[v] == -1) ? (uint64_t)Ddim[lm[v]] : (uint64_t)slen[lch[v]] + slen[rch[v]];
+        if (d.VTptr[v] < 0 || (uint64_t)d.VTptr[v] + (uint64_t)slen[v] * cols > d.VT_len)
+            return fail("projection of node " + std::to_string(v) + " exceeds VT");
+    }
+    if (slen[root] != 0 && lch[root] != -1) {
+        // the reference never projects the root (cacheSkeldim starts at node 1)
+    }
+    VTptr.assign(d.VTptr ? d.VTptr : nullptr, d.VTptr ? d.VTptr + numnodes : nullptr);
+    if (VTptr.empty()) VTptr.assign(numnodes, 0);
+
+    near_x.assign(d.npairx, d.npairx + d.ncount);
+    near_y.assign(d.npairy, d.npairy + d.ncount);
+    near_off.assign(d.Dptr, d.Dptr + d.ncount);
+    for (int k = 0; k < d.ncount; ++k) {
+        const int x = near_x[k], y = near_y[k];
+        if (x < 0 || x >= nleaf || y < 0 || y >= nleaf) return fail("near pair out of range");
+        if (near_off[k] + (uint64_t)Ddim[x] * Ddim[y] > d.D_len) return fail("near block exceeds D");
+    }
+    far_x.assign(d.fpairx, d.fpairx + d.fcount);
+    far_y.assign(d.fpairy, d.fpairy + d.fcount);
+    far_off.assign(d.Bptr, d.Bptr + d.fcount);
+    for (int k = 0; k < d.fcount; ++k) {
+        const int x = far_x[k], y = far_y[k];
+        if (x < 0 || x >= numnodes || y < 0 || y >= numnodes) return fail("far pair out of range");
+        if (x == root || y == root) {
+            if (slen[root] != 0) return fail("far pair touches the root");
+        }
+        if (far_off[k] + (uint64_t)slen[x] * slen[y] > d.B_len) return fail("far block exceeds B");
+    }
+    D_len = d.D_len;
+    B_len = d.B_len;
+    rows_total = 0;
+    leaf_row.resize(nleaf);
+    for (int i = 0; i < nleaf; ++i) {
+        leaf_row[i] = rows_total;
+        rows_total += Ddim[i];
+    }
+    skel_row.assign(numnodes, 0);
+    skel_total = 0;
+    for (int v : bfs) {
+        skel_row[v] = skel_total;
+        skel_total += slen[v];
+    }
+    return MXB_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// task lists
+// ---------------------------------------------------------------------------------------
+
+void Plan::add_task(std::vector<Task> &tasks, int16_t c_kind, int64_t c_row, int ldc, int M,
+                    int item0, int nitem, int16_t beta, int tile)
+{
+    for (int m0 = 0; m0 < M; m0 += tile) {
+        Task t{};
+        t.c_row = c_row;
+        t.ldc = ldc;
+        t.M = M;
+        t.m0 = m0;
+        t.item0 = item0;
+        t.nitem = nitem;
+        t.c_kind = c_kind;
+        t.beta = beta;
+        tasks.push_back(t);
+    }
+}
+
+static Item make_item(int16_t pool, uint64_t a_off, int lda, int K, int trans, int16_t b_kind,
+                      int64_t b_row, int ldb)
+{
+    Item it{};
+    it.a_pool = pool;
+    it.a_off = a_off;
+    it.lda = lda;
+    it.K = K;
+    it.trans = (int16_t)trans;
+    it.b_kind = b_kind;
+    it.b_row = b_row;
+    it.ldb = ldb;
+    return it;
+}
+
+void Plan::build_tasks(int tile)
+{
+    items.clear();
+    tasks.clear();
+    launches_fwd.clear();
+    launches_adj.clear();
+    auto begin_launch = [&](std::vector<Launch> &L, int kind) {
+        Launch l{};
+        l.task0 = (int)tasks.size();
+        l.kind = kind;
+        L.push_back(l);
+    };
+    auto end_launch = [&](std::vector<Launch> &L) {
+        L.back().ntasks = (int)tasks.size() - L.back().task0;
+        if (L.back().ntasks == 0) L.pop_back();
+    };
+    // per-node far lists (forward: pairs (c, y) for output c; adjoint: pairs (x, c))
+    std::vector<std::vector<int>> far_out(numnodes), far_in(numnodes);
+    for (size_t k = 0; k < far_x.size(); ++k) {
+        far_out[far_x[k]].push_back((int)k);
+        far_in[far_y[k]].push_back((int)k);
+    }
+    std::vector<std::vector<int>> near_out(nleaf), near_in(nleaf);
+    for (size_t k = 0; k < near_x.size(); ++k) {
+        near_out[near_x[k]].push_back((int)k);
+        near_in[near_y[k]].push_back((int)k);
+    }
+    int maxh = 0, maxd = 0;
+    for (int v = 0; v < numnodes; ++v) {
+        maxh = std::max(maxh, height[v]);
+        maxd = std::max(maxd, depth[v]);
+    }
+    auto projects = [&](int v) { return v != root && slen[v] > 0; };
+
+    // phases 1-2: up-sweep, shared by forward and adjoint
+    std::vector<Launch> up;
+    for (int h = 0; h <= maxh; ++h) {
+        begin_launch(up, h == 0 ? 1 : 2);
+        for (int v : bfs) {
+            if (height[v] != h || !projects(v)) continue;
+            const int s = slen[v];
+            const int item0 = (int)items.size();
+            if (lch[v] == -1) {
+                const int leaf = lm[v];
+                items.push_back(make_item(2, (uint64_t)VTptr[v], s, Ddim[leaf], 0, KIND_W, leaf, Ddim[leaf]));
+            } else {
+                const int l = lch[v], r = rch[v];
+                if (slen[l] > 0)
+                    items.push_back(make_item(2, (uint64_t)VTptr[v], s, slen[l], 0, KIND_WSKEL, skel_row[l], slen[l]));
+                if (slen[r] > 0)
+                    items.push_back(make_item(2, (uint64_t)VTptr[v] + (uint64_t)s * slen[l], s, slen[r], 0,
+                                              KIND_WSKEL, skel_row[r], slen[r]));
+            }
+            add_task(tasks, KIND_WSKEL, skel_row[v], s, s, item0, (int)items.size() - item0, 0, tile);
+        }
+        end_launch(up);
+    }
+    launches_fwd = up;
+    launches_adj = up;
+
+    // phase 3: far + down, top-down by depth
+    auto down_item = [&](int c) -> bool {
+        const int p = parent[c];
+        if (p < 0 || !projects(p) || slen[c] == 0) return false;
+        const uint64_t off = (uint64_t)VTptr[p] + (c == rch[p] ? (uint64_t)slen[p] * slen[lch[p]] : 0);
+        items.push_back(make_item(2, off, slen[p], slen[p], 1, KIND_USKEL, skel_row[p], slen[p]));
+        return true;
+    };
+    for (int adj = 0; adj < 2; ++adj) {
+        std::vector<Launch> &L = adj ? launches_adj : launches_fwd;
+        for (int dd = 1; dd <= maxd; ++dd) {
+            begin_launch(L, 3);
+            for (int c : bfs) {
+                if (depth[c] != dd || !projects(c)) continue;
+                const int item0 = (int)items.size();
+                if (!adj) {
+                    for (int k : far_out[c]) {
+                        const int y = far_y[k];
+                        if (slen[y] == 0) continue;
+                        items.push_back(make_item(1, far_off[k], slen[c], slen[y], 0, KIND_WSKEL, skel_row[y], slen[y]));
+                    }
+                } else {
+                    for (int k : far_in[c]) {
+                        const int x = far_x[k];
+                        if (slen[x] == 0) continue;
+                        items.push_back(make_item(1, far_off[k], slen[x], slen[x], 1, KIND_WSKEL, skel_row[x], slen[x]));
+                    }
+                }
+                down_item(c);
+                add_task(tasks, KIND_USKEL, skel_row[c], slen[c], slen[c], item0, (int)items.size() - item0, 0, tile);
+            }
+            end_launch(L);
+        }
+        // phase 4: near + leaf down
+        begin_launch(L, 4);
+        for (int v : bfs) {
+            if (lch[v] != -1) continue;
+            const int x = lm[v];
+            const int item0 = (int)items.size();
+            if (!adj) {
+                for (int k : near_out[x]) {
+                    const int y = near_y[k];
+                    items.push_back(make_item(0, near_off[k], Ddim[x], Ddim[y], 0, KIND_W, y, Ddim[y]));
+                }
+            } else {
+                for (int k : near_in[x]) {
+                    const int xx = near_x[k];
+                    items.push_back(make_item(0, near_off[k], Ddim[xx], Ddim[xx], 1, KIND_W, xx, Ddim[xx]));
+                }
+            }
+            if (projects(v)) items.push_back(make_item(2, (uint64_t)VTptr[v], slen[v], slen[v], 1, KIND_USKEL, skel_row[v], slen[v]));
+            add_task(tasks, KIND_Y, x, Ddim[x], Ddim[x], item0, (int)items.size() - item0, 2, tile);
+        }
+        end_launch(L);
+    }
+}
+
+uint64_t Plan::flops(int nrhs) const
+{
+    uint64_t f = 0;
+    for (int v = 0; v < numnodes; ++v) {
+        if (v == root) continue;
+        const uint64_t s = (uint64_t)slen[v];
+        if (lch[v] == -1) f += 2 * s * nrhs * (uint64_t)Ddim[lm[v]];
+        else f += 2 * s * ((uint64_t)slen[lch[v]] + slen[rch[v]]) * nrhs;
+    }
+    f *= 2;
+    for (size_t k = 0; k < near_x.size(); ++k) f += 2ull * Ddim[near_x[k]] * Ddim[near_y[k]] * nrhs;
+    for (size_t k = 0; k < far_x.size(); ++k) f += 2ull * slen[far_x[k]] * slen[far_y[k]] * nrhs;
+    return f;
+}
+
+// ---------------------------------------------------------------------------------------
+// creation, scratch, evaluation
+// ---------------------------------------------------------------------------------------
+
+int Plan::create(const mxb_cds_desc &d, int prec, Plan **out)
+{
+    if (prec != MXB_PREC_FP64 && prec != MXB_PREC_SPLIT_BF16) {
+        set_error("unknown precision mode");
+        return MXB_ERR_ARG;
+    }
+    std::unique_ptr<Plan> p(new Plan());
+    p->precision = prec;
+    MXB_CUDA(cudaGetDevice(&p->device));
+    int rc = p->validate(d);
+    if (rc) return rc;
+    p->build_tasks(row_tile_for(prec));
+    // FP64 CDS
+    rc = p->alloc((void **)&p->dD, std::max<uint64_t>(d.D_len, 1) * sizeof(double));
+    if (rc) return rc;
+    MXB_CUDA(cudaMemcpy(p->dD, d.D, d.D_len * sizeof(double), cudaMemcpyHostToDevice));
+    rc = p->alloc((void **)&p->dB, std::max<uint64_t>(d.B_len, 1) * sizeof(double));
+    if (rc) return rc;
+    if (d.B_len) MXB_CUDA(cudaMemcpy(p->dB, d.B, d.B_len * sizeof(double), cudaMemcpyHostToDevice));
+    rc = p->alloc((void **)&p->dVT, std::max<uint64_t>(d.VT_len, 1) * sizeof(double));
+    if (rc) return rc;
+    if (d.VT_len) MXB_CUDA(cudaMemcpy(p->dVT, d.VT, d.VT_len * sizeof(double), cudaMemcpyHostToDevice));
+    rc = p->alloc((void **)&p->dTasks, p->tasks.size() * sizeof(Task));
+    if (rc) return rc;
+    if (!p->tasks.empty())
+        MXB_CUDA(cudaMemcpy(p->dTasks, p->tasks.data(), p->tasks.size() * sizeof(Task), cudaMemcpyHostToDevice));
+    rc = p->alloc((void **)&p->dItems, p->items.size() * sizeof(Item));
+    if (rc) return rc;
+    if (!p->items.empty())
+        MXB_CUDA(cudaMemcpy(p->dItems, p->items.data(), p->items.size() * sizeof(Item), cudaMemcpyHostToDevice));
+    rc = p->alloc((void **)&p->dOfs, 4 * (size_t)p->nleaf * sizeof(int32_t));
+    if (rc) return rc;
+    if (prec == MXB_PREC_SPLIT_BF16) {
+        rc = p->setup_split_bf16(d);
+        if (rc) return rc;
+    }
+    *out = p.release();
+    return MXB_OK;
+}
+
+int Plan::ensure_scratch(int nrhs)
+{
+    const size_t need = (size_t)std::max<int64_t>(skel_total, 1) * nrhs;
+    if (need <= scratch_elems) return MXB_OK;
+    if (dWskel) {
+        cudaFree(dWskel);
+        cudaFree(dUskel);
+        allocations.erase(std::remove(allocations.begin(), allocations.end(), (void *)dWskel), allocations.end());
+        allocations.erase(std::remove(allocations.begin(), allocations.end(), (void *)dUskel), allocations.end());
+        device_bytes -= 2 * scratch_elems * sizeof(double);
+        dWskel = dUskel = nullptr;
+        scratch_elems = 0;
+    }
+    int rc = alloc((void **)&dWskel, need * sizeof(double));
+    if (rc) return rc;
+    rc = alloc((void **)&dUskel, need * sizeof(double));
+    if (rc) return rc;
+    scratch_elems = need;
+    return MXB_OK;
+}
+
+// Per-leaf offsets for one call; packed offsets when the caller passes none.
+int Plan::stage_offsets(int slot, const int32_t *ofs, int nrhs, cudaStream_t stream)
+{
+    std::vector<int32_t> &host = ofs_host[slot];
+    std::vector<int32_t> want(nleaf);
+    if (ofs) {
+        std::memcpy(want.data(), ofs, sizeof(int32_t) * nleaf);
+        for (int i = 0; i < nleaf; ++i)
+            if (want[i] < 0) return fail("negative leaf offset");
+    } else {
+        for (int i = 0; i < nleaf; ++i) {
+            const int64_t o = leaf_row[i] * (int64_t)nrhs;
+            if (o > INT32_MAX) return fail("packed leaf offsets overflow int32");
+            want[i] = (int32_t)o;
+        }
+    }
+    if (want != host) {
+        host = want;
+        MXB_CUDA(cudaMemcpyAsync(dOfs + (size_t)slot * nleaf, host.data(), sizeof(int32_t) * nleaf,
+                                 cudaMemcpyHostToDevice, stream));
+        MXB_CUDA(cudaStreamSynchronize(stream));
+    }
+    return MXB_OK;
+}
+
+int Plan::run(const std::vector<Launch> &L, const double *dW, double *dY, int nrhs,
+              const int32_t *wofs, const int32_t *yofs, int accumulate, cudaStream_t stream)
+{
+    if (nrhs < 1) {
+        set_error("nrhs must be >= 1");
+        return MXB_ERR_ARG;
+    }
+    if (!dW || !dY) {
+        set_error("null device operand");
+        return MXB_ERR_ARG;
+    }
+    int cur = -1;
+    MXB_CUDA(cudaGetDevice(&cur));
+    if (cur != device) {
+        set_error("plan used on a different device than it was created on");
+        return MXB_ERR_ARG;
+    }
+    int rc = ensure_scratch(nrhs);
+    if (rc) return rc;
+    rc = stage_offsets(0, wofs, nrhs, stream);
+    if (rc) return rc;
+    rc = stage_offsets(1, yofs, nrhs, stream);
+    if (rc) return rc;
+    if (precision == MXB_PREC_SPLIT_BF16) return run_split_bf16(L, dW, dY, nrhs, accumulate, stream);
+    Operands ops{};
+    ops.pool[0] = dD;
+    ops.pool[1] = dB;
+    ops.pool[2] = dVT;
+    ops.W = dW;
+    ops.Y = dY;
+    ops.wskel = dWskel;
+    ops.uskel = dUskel;
+    ops.wofs = dOfs;
+    ops.yofs = dOfs + nleaf;
+    ops.nrhs = nrhs;
+    ops.beta_arg = accumulate ? 1 : 0;
+    for (const Launch &l : L) {
+        cudaError_t e = launch_gemm_f64(dTasks + l.task0, dItems, l.ntasks, ops, stream);
+        if (e != cudaSuccess) {
+            set_error(std::string("FP64 grouped GEMM launch: ") + cudaGetErrorString(e));
+            return MXB_ERR_CUDA;
+        }
+    }
+    return MXB_OK;
+}
+
+int Plan::read_workspaces(int nrhs, const int32_t *wsko, double *wskel, const int32_t *usko, double *uskel)
+{
+    if (!dWskel || scratch_elems < (size_t)skel_total * nrhs) {
+        set_error("no evaluation with this nrhs has run on the plan");
+        return MXB_ERR_ARG;
+    }
+    MXB_CUDA(cudaDeviceSynchronize());
+    std::vector<double> w((size_t)skel_total * nrhs), u((size_t)skel_total * nrhs);
+    MXB_CUDA(cudaMemcpy(w.data(), dWskel, w.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    MXB_CUDA(cudaMemcpy(u.data(), dUskel, u.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int v = 0; v < numnodes; ++v) {
+        const size_t n = (size_t)slen[v] * nrhs;
+        if (!n) continue;
+        if (wskel && wsko) std::memcpy(wskel + wsko[v], w.data() + skel_row[v] * nrhs, n * sizeof(double));
+        if (uskel && usko) std::memcpy(uskel + usko[v], u.data() + skel_row[v] * nrhs, n * sizeof(double));
+    }
+    return MXB_OK;
+}
+
+}  // namespace mxb

@@ -1,0 +1,325 @@
+"""Host-side mirror of MatRox's evaluator interface over the C-ABI.
+
+* :func:`CBHGEMM`, :func:`HGEMM`, :func:`parHSSGEMM` ... call the drop-ins with the
+  reference's argument lists, built from a :class:`~matrox_ru_b200.structure.CDS` the way
+  ``matroxTest-V1/main.cpp:97-107`` and ``codeTest/main.cpp:111-171`` build them.
+* :class:`Plan` wraps the device-pointer plan API for torch tensors.
+* :class:`Evaluator` adds the permutation between the caller's point order and the
+  leaf-blocked tree order, and the adjoint.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import P, I32, check
+
+PRECISIONS = {"fp64": _lib.PREC_FP64, "split_bf16": _lib.PREC_SPLIT_BF16}
+
+
+def _np(a, dt):
+    a = np.ascontiguousarray(a, dtype=dt)
+    if a.size == 0:
+        a = np.zeros(1, dt)
+    return a
+
+
+class _Args:
+    """Keeps the numpy arrays of one drop-in call alive and hands out their pointers."""
+
+    def __init__(self):
+        self.keep = []
+
+    def __call__(self, a, dt=np.int32):
+        a = _np(a, dt)
+        self.keep.append(a)
+        return a.ctypes.data_as(P)
+
+
+def set_precision(mode: str) -> None:
+    check(_lib.load().mxb_set_precision(PRECISIONS[mode]), "mxb_set_precision")
+
+
+def set_flags(flags: int) -> None:
+    check(_lib.load().mxb_set_flags(flags), "mxb_set_flags")
+
+
+def cache_invalidate() -> None:
+    check(_lib.load().mxb_cache_invalidate(), "mxb_cache_invalidate")
+
+
+def _ref_args(cds, TW, apres, nrhs, wskel, uskel, idx):
+    a = _Args()
+    wptr, uptr, wsko, usko, _ = cds.offsets(nrhs)
+    args = [a(cds.D, np.float64), a(cds.B, np.float64), a(cds.VT, np.float64), a(cds.Dptr, np.uint64),
+            a(cds.Bptr, np.uint64), a(cds.VTptr), a(cds.lchildren), a(cds.rchildren), a(cds.levelset),
+            a(idx), TW.ctypes.data_as(P), apres.ctypes.data_as(P), I32(nrhs), a(cds.Ddim), a(wptr),
+            a(uptr), wskel.ctypes.data_as(P), a(wsko), uskel.ctypes.data_as(P), a(usko), a(cds.lm),
+            a(cds.slen)]
+    return a, args
+
+
+def _work(cds, nrhs, wskel, uskel):
+    n = max(int(cds.slen.astype(np.int64).sum()) * nrhs, 1)
+    if wskel is None:
+        wskel = np.zeros(n)
+    if uskel is None:
+        uskel = np.zeros(n)
+    return wskel, uskel
+
+
+def CBHGEMM(cds, TW: np.ndarray, apres: np.ndarray, nrhs: int, wskel=None, uskel=None,
+            variant: str = "CBHGEMM") -> int:
+    """Drop-in H2-b evaluation on host arrays (``codeGen/H2GEMM.h:380``):
+    apres += K~ TW, both leaf-blocked FP64 arrays of N * nrhs elements."""
+    if cds.is_hss:
+        raise ValueError("CBHGEMM takes an H2-b CDS; use parHSSGEMM for HSS")
+    lib = _lib.load()
+    wskel, uskel = _work(cds, nrhs, wskel, uskel)
+    idx = cds.idx if variant == "blockGEMM" else cds.cidx
+    a, args = _ref_args(cds, TW, apres, nrhs, wskel, uskel, idx)
+    args += [a(cds.nblockset), a(cds.nblocks), a(cds.npairx), a(cds.npairy), a(cds.fblockset),
+             a(cds.fblocks), a(cds.fpairx), a(cds.fpairy)]
+    if variant in ("CBHGEMM", "lowH2GEMM"):
+        args += [I32(cds.nrow), I32(cds.frow), a(cds.wpart), a(cds.clevelset), ctypes.c_int(cds.cdepth)]
+        rc = getattr(lib, variant)(*args)
+    elif variant == "blockGEMM":
+        args += [I32(cds.nrow), I32(cds.frow), I32(cds.depth)]
+        rc = lib.blockGEMM(*args)
+    elif variant == "HGEMM":
+        check(lib.mxb_hgemm_set_shape(cds.nrow, cds.frow, cds.cdepth), "mxb_hgemm_set_shape")
+        args += [a(cds.wpart), a(cds.clevelset)]
+        rc = lib.HGEMM(*args)
+    else:
+        raise ValueError(variant)
+    check(rc, variant)
+    return rc
+
+
+def parHSSGEMM(cds, TW: np.ndarray, apres: np.ndarray, nrhs: int, wskel=None, uskel=None,
+               variant: str = "parHSSGEMM") -> int:
+    """Drop-in HSS evaluation on host arrays (``codeGen/HSSGEMM.h:131``):
+    apres = K~ TW (the HSS near pass overwrites)."""
+    if not cds.is_hss:
+        raise ValueError("parHSSGEMM takes an HSS CDS")
+    lib = _lib.load()
+    wskel, uskel = _work(cds, nrhs, wskel, uskel)
+    idx = cds.idx if variant == "seqHSSGEMM" else cds.cidx
+    a, args = _ref_args(cds, TW, apres, nrhs, wskel, uskel, idx)
+    if variant in ("parHSSGEMM", "lowHSSGEMM"):
+        args += [a(cds.wpart), a(cds.clevelset), ctypes.c_int(cds.nleaf), ctypes.c_int(cds.numnodes - 1),
+                 ctypes.c_int(cds.cdepth)]
+        rc = getattr(lib, variant)(*args)
+    elif variant == "seqHSSGEMM":
+        args += [I32(cds.nleaf), I32(cds.numnodes - 1), I32(cds.depth)]
+        rc = lib.seqHSSGEMM(*args)
+    elif variant == "HGEMM_HSS":
+        check(lib.mxb_hgemm_hss_set_shape(cds.nleaf, cds.cdepth), "mxb_hgemm_hss_set_shape")
+        args += [a(cds.wpart), a(cds.clevelset)]
+        rc = lib.HGEMM_HSS(*args)
+    else:
+        raise ValueError(variant)
+    check(rc, variant)
+    return rc
+
+
+def evaluate_host(cds, TW: np.ndarray, nrhs: int, apres: Optional[np.ndarray] = None) -> np.ndarray:
+    """Reference-style host call of whichever drop-in matches the CDS (apres zeroed if None)."""
+    TW = np.ascontiguousarray(TW, dtype=np.float64)
+    if apres is None:
+        apres = np.zeros_like(TW)
+    (parHSSGEMM if cds.is_hss else CBHGEMM)(cds, TW, apres, nrhs)
+    return apres
+
+
+def transform(cds, W: np.ndarray, nrhs: int) -> np.ndarray:
+    """``transform`` (``hcds.h:766``) on the GPU: W (N x nrhs, column-major) -> TW."""
+    lib = _lib.load()
+    W = np.asfortranarray(W, dtype=np.float64)
+    wptr = cds.offsets(nrhs)[0]
+    TW = np.zeros(cds.n * nrhs)
+    a = _Args()
+    check(lib.mxb_transform(a(cds.perm), a(cds.leaf_lids_offset), a(wptr), cds.nleaf, W.ctypes.data_as(P),
+                            cds.n, cds.n, nrhs, TW.ctypes.data_as(P)), "mxb_transform")
+    return TW
+
+
+def untransform(cds, TY: np.ndarray, nrhs: int) -> np.ndarray:
+    lib = _lib.load()
+    uptr = cds.offsets(nrhs)[1]
+    Y = np.zeros((cds.n, nrhs), order="F")
+    a = _Args()
+    check(lib.mxb_untransform(a(cds.perm), a(cds.leaf_lids_offset), a(uptr), cds.nleaf,
+                              a(TY, np.float64), cds.n, cds.n, nrhs, Y.ctypes.data_as(P)), "mxb_untransform")
+    return Y
+
+
+# -----------------------------------------------------------------------------------------
+# device plans (torch tensors)
+# -----------------------------------------------------------------------------------------
+
+def _torch():
+    import torch
+    return torch
+
+
+def _stream_ptr(stream) -> int:
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream
+
+
+def cds_desc(cds, keep: list) -> _lib.CdsDesc:
+    def k(a, dt=np.int32):
+        a = _np(a, dt)
+        keep.append(a)
+        return a.ctypes.data
+
+    d = _lib.CdsDesc()
+    d.nleaf, d.numnodes, d.is_hss = cds.nleaf, cds.numnodes, int(cds.is_hss)
+    d.D, d.D_len = k(cds.D, np.float64), cds.D.size
+    d.B, d.B_len = k(cds.B, np.float64), cds.B.size
+    d.VT, d.VT_len = k(cds.VT, np.float64), cds.VT.size
+    d.Dptr, d.Bptr, d.VTptr = k(cds.Dptr, np.uint64), k(cds.Bptr, np.uint64), k(cds.VTptr)
+    d.lchildren, d.rchildren, d.lm, d.slen, d.Ddim = (k(cds.lchildren), k(cds.rchildren), k(cds.lm),
+                                                      k(cds.slen), k(cds.Ddim))
+    d.npairx, d.npairy, d.ncount = k(cds.npairx), k(cds.npairy), cds.ncount
+    d.fpairx, d.fpairy, d.fcount = k(cds.fpairx), k(cds.fpairy), cds.fcount
+    return d
+
+
+class Plan:
+    """Device-resident CDS and task lists (``mxb_plan_*``)."""
+
+    def __init__(self, cds, precision: str = "fp64"):
+        torch = _torch()
+        if not torch.cuda.is_available():
+            raise RuntimeError("matrox_ru_b200.Plan needs a CUDA device")
+        lib = _lib.load()
+        keep: list = []
+        desc = cds_desc(cds, keep)
+        h = P()
+        check(lib.mxb_plan_create(ctypes.byref(desc), PRECISIONS[precision], ctypes.byref(h)), "mxb_plan_create")
+        self._h = h
+        self.cds = cds
+        self.precision = precision
+        self.n = cds.n
+        self.device = torch.cuda.current_device()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().mxb_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def flops(self, nrhs: int) -> int:
+        f = _lib.U64()
+        check(_lib.load().mxb_plan_flops(self._h, nrhs, ctypes.byref(f)), "mxb_plan_flops")
+        return int(f.value)
+
+    def info(self):
+        b, l, p = _lib.U64(), I32(), I32()
+        check(_lib.load().mxb_plan_info(self._h, ctypes.byref(b), ctypes.byref(l), ctypes.byref(p)), "mxb_plan_info")
+        return {"device_bytes": int(b.value), "launches": int(l.value), "precision": int(p.value)}
+
+    def _check_operand(self, t, nrhs):
+        torch = _torch()
+        if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
+            raise TypeError("operands must be contiguous float64 CUDA tensors")
+        if t.numel() < self.n * nrhs:
+            raise ValueError("operand smaller than N * nrhs")
+
+    def evaluate(self, TW, nrhs: int, out=None, accumulate: bool = False, stream=None):
+        """out (+)= K~ TW on packed leaf-blocked float64 CUDA tensors (N * nrhs)."""
+        torch = _torch()
+        self._check_operand(TW, nrhs)
+        if out is None:
+            out = torch.zeros(self.n * nrhs, dtype=torch.float64, device=TW.device)
+            accumulate = False
+        self._check_operand(out, nrhs)
+        check(_lib.load().mxb_plan_evaluate(self._h, TW.data_ptr(), out.data_ptr(), nrhs, None, None,
+                                            int(accumulate), _stream_ptr(stream)), "mxb_plan_evaluate")
+        return out
+
+    def adjoint(self, TG, nrhs: int, out=None, accumulate: bool = False, stream=None):
+        """out (+)= K~^T TG (packed leaf-blocked float64 CUDA tensors)."""
+        torch = _torch()
+        self._check_operand(TG, nrhs)
+        if out is None:
+            out = torch.zeros(self.n * nrhs, dtype=torch.float64, device=TG.device)
+            accumulate = False
+        self._check_operand(out, nrhs)
+        check(_lib.load().mxb_plan_adjoint(self._h, TG.data_ptr(), out.data_ptr(), nrhs, None, None,
+                                           int(accumulate), _stream_ptr(stream)), "mxb_plan_adjoint")
+        return out
+
+
+class Evaluator:
+    """Y = K~ W with W, Y as (N, r) float64 CUDA tensors in the caller's point order."""
+
+    def __init__(self, cds, precision: str = "fp64"):
+        torch = _torch()
+        self.plan = Plan(cds, precision)
+        self.cds = cds
+        dev = torch.device("cuda", self.plan.device)
+        self.perm = torch.as_tensor(cds.perm.astype(np.int32), device=dev)
+        self.leafofs = torch.as_tensor(cds.leaf_lids_offset.astype(np.int32), device=dev)
+        self._blockofs = {}
+
+    def blockofs(self, nrhs: int):
+        if nrhs not in self._blockofs:
+            torch = _torch()
+            offs = (self.cds.leaf_lids_offset[:-1].astype(np.int64) * nrhs)
+            if offs.size and offs[-1] > np.iinfo(np.int32).max:
+                raise ValueError("leaf offsets overflow int32")
+            self._blockofs[nrhs] = torch.as_tensor(offs.astype(np.int32), device=self.perm.device)
+        return self._blockofs[nrhs]
+
+    def to_tree(self, W, stream=None):
+        torch = _torch()
+        n, r = W.shape
+        TW = torch.empty(n * r, dtype=torch.float64, device=W.device)
+        check(_lib.load().mxb_permute_rows(self.perm.data_ptr(), self.leafofs.data_ptr(),
+                                           self.blockofs(r).data_ptr(), self.cds.nleaf, n, W.data_ptr(),
+                                           TW.data_ptr(), W.stride(0), W.stride(1), r, 0, 0,
+                                           _stream_ptr(stream)), "mxb_permute_rows")
+        return TW
+
+    def from_tree(self, TY, r, out=None, accumulate=False, stream=None):
+        torch = _torch()
+        n = self.cds.n
+        if out is None:
+            out = torch.empty((n, r), dtype=torch.float64, device=TY.device)
+            accumulate = False
+        check(_lib.load().mxb_permute_rows(self.perm.data_ptr(), self.leafofs.data_ptr(),
+                                           self.blockofs(r).data_ptr(), self.cds.nleaf, n, TY.data_ptr(),
+                                           out.data_ptr(), out.stride(0), out.stride(1), r, 1, int(accumulate),
+                                           _stream_ptr(stream)), "mxb_permute_rows")
+        return out
+
+    def __call__(self, W, stream=None):
+        torch = _torch()
+        if W.dtype != torch.float64 or not W.is_cuda or W.dim() != 2 or W.shape[0] != self.cds.n:
+            raise TypeError("W must be an (N, r) float64 CUDA tensor")
+        r = W.shape[1]
+        TY = self.plan.evaluate(self.to_tree(W, stream), r, stream=stream)
+        return self.from_tree(TY, r, stream=stream)
+
+    def adjoint(self, G, stream=None):
+        r = G.shape[1]
+        TGW = self.plan.adjoint(self.to_tree(G, stream), r, stream=stream)
+        return self.from_tree(TGW, r, stream=stream)
+
+
+def kernel_matvec(evaluator: Evaluator, W):
+    """Differentiable Y = K~ W (gradient by the transposed traversal)."""
+    from .autograd import KernelMatVec
+    return KernelMatVec.apply(W, evaluator)
