@@ -1,0 +1,390 @@
+#!/usr/bin/env python
+"""Benchmark of Y = K~ W on one B200 per rank: the H2-b compressed Gaussian kernel matrix of
+N = 65536 points in d = 28 (16-component mixture, h = 2, leaf 256, budget 0.03, ID tolerance
+1e-5, max rank 256) times W with 1024 right-hand sides.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  Under torchrun every rank evaluates its own W against the
+same CDS (weak scaling, no collective on the data path; one scalar max-reduce for timing).
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import io
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "K~W ms & roofline %: FP64 vs split-BF16 at <=1e-5 rel err, N=65536, 1024 rhs"
+WORKLOAD = dict(workload="H2-b K~W, N=65536 d=28 gaussian-mixture(16), h=2.0, leaf 256, budget 0.03, "
+                         "tol 1e-5, max rank 256, nrhs 1024",
+                n=65536, d=28, components=16, mean_range=[-2.0, 2.0], sigma_range=[0.3, 1.0], kernel="gaussian",
+                h=2.0, leaf=256, budget=0.03, tol=1e-5, max_rank=256, nrhs=1024, seed=20261203)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["fp64", "split_bf16", "both"], default="both")
+    ap.add_argument("--n", type=int, default=None, help="override N (small smoke runs only)")
+    ap.add_argument("--nrhs", type=int, default=None)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def build_cds(cfg):
+    from matrox_ru_b200 import structure as S
+    X = S.gaussian_mixture(cfg["n"], cfg["d"], cfg["components"], *cfg["mean_range"], *cfg["sigma_range"],
+                           seed=cfg["seed"])
+    t = time.time()
+    cds = S.build_cds(X, S.KernelSpec(cfg["kernel"], cfg["h"]), leaf_size=cfg["leaf"], budget=cfg["budget"],
+                      tol=cfg["tol"], max_rank=cfg["max_rank"], seed=cfg["seed"])
+    return X, cds, time.time() - t
+
+
+def leaf_slice(cds, TW, r_full, r):
+    """First r columns of every leaf block of a packed leaf-blocked array (r_full columns)."""
+    out = np.empty(cds.n * r)
+    for i in range(cds.nleaf):
+        a, b = int(cds.leaf_lids_offset[i]), int(cds.leaf_lids_offset[i + 1])
+        m = b - a
+        out[a * r:a * r + m * r] = TW[a * r_full:a * r_full + m * r]
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.rows = []
+        if self.p is None:
+            return
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            out, _ = self.p.communicate(timeout=5)
+        except Exception:
+            self.p.kill()
+            out = ""
+        for row in csv.reader(io.StringIO(out)):
+            if len(row) >= 9:
+                self.rows.append([c.strip() for c in row])
+
+    def summary(self):
+        if not getattr(self, "rows", None):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def fp64_peak_tflops(torch, dev):
+    """Measured denominator for the FP64 path: cuBLAS DGEMM 8192^3 (best of 5)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+def profile_traffic():
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {}
+
+
+def run_reference(args, cfg, rank):
+    """--impl reference: the reference's own CBHGEMM (codeGen/H2GEMM.h:380) compiled from its
+    sources into oracle/_ref, on all host cores, full workload per step."""
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libmatrox_ref.so was not built "
+                          "(the reference tree was absent at build time)"}))
+        return
+    X, cds, tb = build_cds(cfg)
+    r = cfg["nrhs"]
+    rng = np.random.default_rng(cfg["seed"] + 1)
+    TW = rng.standard_normal(cds.n * r)
+    lib = O.ref()
+    cores = os.cpu_count() or 1
+    lib.ref_set_omp_threads(cores)
+    lib.ref_set_blas_threads(1)
+    ws = O.Workspace(cds, r)
+    Y = np.zeros_like(TW)
+    for _ in range(args.warmup):
+        O.eval_h2b(cds, TW, r, Y=Y, use_reference=True, ws=ws)
+    times = []
+    for _ in range(args.steps):
+        Y[:] = 0
+        t0 = time.perf_counter()
+        O.eval_h2b(cds, TW, r, Y=Y, use_reference=True, ws=ws)
+        times.append(time.perf_counter() - t0)
+    ms = 1e3 * float(np.median(times))
+    flops = cds.flops(r)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(ms, 3), "unit": "ms", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(WORKLOAD, flops_per_eval=flops, inputs="larger than L2 (W 512 MiB, CDS > 2 GiB)"),
+        "gflops": round(flops / (ms * 1e-3) / 1e9, 2),
+        "cpu_baseline": {"value": round(ms, 3), "unit": "ms", "cores": cores, "kind": "reference",
+                         "sample": f"full workload per step ({r} rhs), median of {args.steps}; CBHGEMM "
+                                   f"(codeGen/H2GEMM.h) over OpenBLAS, OMP threads={cores}"},
+        "e2e": {"value": round(ms, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "cds_build_s": round(tb, 1),
+    }
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    cfg = dict(WORKLOAD)
+    if args.n:
+        cfg["n"] = args.n
+    if args.nrhs:
+        cfg["nrhs"] = args.nrhs
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if world > 1:
+            import torch.distributed as dist
+            dist.init_process_group("gloo")
+            dist.barrier()
+            run_reference(args, cfg, rank)
+            dist.barrier()
+            dist.destroy_process_group()
+        else:
+            run_reference(args, cfg, rank)
+        return
+
+    import torch
+    from matrox_ru_b200 import build as mbuild, hgemm as H, _lib
+    mbuild.build()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+
+    X, cds, t_build = build_cds(cfg)
+    r = cfg["nrhs"]
+    flops = cds.flops(r)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(cfg["seed"] + 1 + rank)
+    TW = torch.randn(cds.n * r, dtype=torch.float64, device=dev, generator=gen)
+    peaks, peak_src = measured_peaks()
+    fp64_peak = fp64_peak_tflops(torch, dev)
+
+    modes = ["fp64", "split_bf16"] if args.precision == "both" else [args.precision]
+    results = {}
+    clocks = None
+    stream = torch.cuda.current_stream()
+    for mode in modes:
+        try:
+            plan = H.Plan(cds, mode)
+        except _lib.MxbError as e:
+            if e.code == _lib.MXB_ERR_UNSUPPORTED:
+                results[mode] = {"unavailable": str(e)}
+                continue
+            raise
+        out = torch.zeros(cds.n * r, dtype=torch.float64, device=dev)
+        for _ in range(max(args.warmup, 3)):
+            plan.evaluate(TW, r, out=out)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        with ClockSampler(local) as cs:
+            for e0, e1 in ev:
+                e0.record(stream)
+                plan.evaluate(TW, r, out=out)
+                e1.record(stream)
+            torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        per = [e0.elapsed_time(e1) for e0, e1 in ev]
+        ms = float(np.sum(per)) / len(per)
+        if dist:
+            t = torch.tensor([ms], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        info = plan.info()
+        res = {"ms": round(ms, 4), "gflops": round(flops / (ms * 1e-3) / 1e9, 1), "launches_per_eval": info["launches"],
+               "device_bytes": info["device_bytes"], "step_ms_min": round(min(per), 4),
+               "step_ms_max": round(max(per), 4), "clocks": cs.summary()}
+        # accuracy on this CDS: vs the reference's FP64 evaluation (16-column slice) and vs dense
+        if rank == 0:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import oracle as O
+            rc = 16
+            TWs = leaf_slice(cds, TW.cpu().numpy(), r, rc)
+            Ys = leaf_slice(cds, out.cpu().numpy(), r, rc)
+            if O.ref_available():
+                Yref = O.eval_h2b(cds, TWs, rc, use_reference=True)
+                res["rel_err_vs_reference_same_cds"] = float(np.linalg.norm(Ys - Yref) / np.linalg.norm(Yref))
+                res["max_rel_err_vs_reference_same_cds"] = float(np.abs(Ys - Yref).max() / np.abs(Yref).max())
+            from matrox_ru_b200 import structure as S
+            rows = np.random.default_rng(0).choice(cds.n, 64, replace=False)
+            Wo = cds.from_tree_order(TWs, rc)
+            Yd = S.dense_kernel_times(X, Wo, S.KernelSpec(cfg["kernel"], cfg["h"]), rows=rows)
+            Yo = cds.from_tree_order(Ys, rc)[rows]
+            res["rel_err_vs_dense_64rows"] = float(np.linalg.norm(Yo - Yd) / np.linalg.norm(Yd))
+        results[mode] = res
+        if clocks is None:
+            clocks = res["clocks"]
+        del plan, out
+        torch.cuda.empty_cache()
+
+    ok = {m: v for m, v in results.items() if "ms" in v and
+          (m == "fp64" or v.get("rel_err_vs_reference_same_cds", 1.0) <= 1e-5)}
+    best = min(ok, key=lambda m: ok[m]["ms"])
+    head = ok[best]
+    ms = head["ms"]
+
+    # roofline of the dominant kernel (the grouped GEMM: every launch of an evaluation)
+    traffic = profile_traffic().get(best)
+    if best == "fp64":
+        roof = {"bound": "tensor", "achieved": round(flops / (ms * 1e-3) / 1e12, 3), "peak": round(fp64_peak, 2),
+                "unit": "TFLOP/s", "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 (torch.matmul f64)",
+                "kernel": "gemm_f64_kernel (all launches of one evaluation)",
+                "per_launch_flops": flops // max(head["launches_per_eval"], 1)}
+    else:
+        roof = {"bound": "tensor", "achieved": round(head.get("executed_flops", flops) / (ms * 1e-3) / 1e12, 3),
+                "peak": peaks["bf16_tflops"], "unit": "TFLOP/s", "peak_source": f"MEASURED_PEAKS.json bf16 ({peak_src})"}
+    roof["frac"] = round(roof["achieved"] / roof["peak"], 4)
+    roof["traffic"] = traffic
+
+    # end to end through the reference-signature drop-in, host buffers (pinned)
+    e2e = None
+    if not args.no_e2e:
+        H.set_precision(best)
+        H.set_flags(0)
+        pin_tw = torch.empty(cds.n * r, dtype=torch.float64, pin_memory=True)
+        pin_tw.copy_(TW.cpu())
+        pin_y = torch.zeros(cds.n * r, dtype=torch.float64, pin_memory=True)
+        tw_np, y_np = pin_tw.numpy(), pin_y.numpy()
+        for _ in range(2):
+            H.evaluate_host(cds, tw_np, r, apres=y_np)
+        if dist:
+            dist.barrier()
+        times = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            H.evaluate_host(cds, tw_np, r, apres=y_np)
+            times.append(time.perf_counter() - t0)
+        e2e_ms = 1e3 * float(np.mean(times))
+        if dist:
+            t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        nb = cds.n * r * 8
+        e2e = {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": 2 * nb, "d2h_bytes_per_step": nb,
+               "api": "CBHGEMM drop-in (reference signature, host arrays, synchronous)"}
+        H.cache_invalidate()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        if O.ref_available():
+            rs = min(256, r)
+            TWs = leaf_slice(cds, TW.cpu().numpy(), r, rs)
+            lib = O.ref()
+            cores = os.cpu_count() or 1
+            lib.ref_set_omp_threads(cores)
+            ws = O.Workspace(cds, rs)
+            O.eval_h2b(cds, TWs, rs, use_reference=True, ws=ws)
+            ts = []
+            for _ in range(3):
+                t0 = time.perf_counter()
+                O.eval_h2b(cds, TWs, rs, use_reference=True, ws=ws)
+                ts.append(time.perf_counter() - t0)
+            cpu_ms = 1e3 * float(np.median(ts)) * (r / rs)
+            cpu = {"value": round(cpu_ms, 1), "unit": "ms", "cores": cores, "kind": "reference",
+                   "sample": f"reference CBHGEMM on the same CDS with the first {rs} of {r} rhs, median of 3, "
+                             f"scaled by {r}/{rs} (flops are linear in nrhs)"}
+
+    launches = head["launches_per_eval"] * args.steps
+    line = {
+        "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if best == "fp64" else "bf16x3(split)+f32+f64", "data": "synthetic",
+        "config": dict(cfg, precision=best, flops_per_eval=flops,
+                       inputs="larger than L2: W 512 MiB and CDS > 2 GiB read every step",
+                       parallelism=f"replicas x{world} (weak scaling; no data-path collective)"),
+        "gflops": round(flops / (ms * 1e-3) / 1e9, 1),
+        "aggregate_gflops": round(world * flops / (ms * 1e-3) / 1e9, 1),
+        "modes": results, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+        "clocks": clocks, "cds_build_s": round(t_build, 1),
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -31,8 +31,11 @@ the reference's randomised-tree 32-NN search; the tree split fills a perfect tre
 """
 from __future__ import annotations
 
+import contextlib
 import dataclasses
 import math
+import os
+from concurrent.futures import ThreadPoolExecutor
 from typing import Dict, List, Optional, Tuple
 
 import numpy as np
@@ -562,30 +565,43 @@ class CDS:
 # compression driver
 # ---------------------------------------------------------------------------
 
-def _sample_rows(X, own: np.ndarray, cand: np.ndarray, nsamples: int, n: int,
+def _workers() -> int:
+    return max(1, min(32, os.cpu_count() or 1))
+
+
+@contextlib.contextmanager
+def _blas_single_thread():
+    try:
+        from threadpoolctl import threadpool_limits
+    except Exception:  # pragma: no cover
+        yield
+        return
+    with threadpool_limits(limits=1, user_api="blas"):
+        yield
+
+def _sample_rows(own: np.ndarray, cand: np.ndarray, nsamples: int, n: int,
                  rng: np.random.Generator) -> np.ndarray:
     """Rows for the ID of a node: nearest outside candidates first (up to half of
     ``nsamples``), then uniform random outside points (``compression.h:597-690``)."""
     if nsamples >= n - len(own):
         return np.arange(n, dtype=np.int64)
-    owns = set(own.tolist())
-    picked: List[int] = []
-    seen = set()
-    for c in cand.tolist():
-        if len(picked) >= nsamples // 2:
-            break
-        if c not in owns and c not in seen:
-            picked.append(c)
-            seen.add(c)
-    while len(picked) < nsamples:
-        draw = rng.integers(0, n, size=2 * (nsamples - len(picked)) + 8)
-        for c in draw.tolist():
-            if c not in owns and c not in seen:
-                picked.append(c)
-                seen.add(c)
-                if len(picked) >= nsamples:
-                    break
-    return np.array(picked, dtype=np.int64)
+    taken = np.zeros(n, bool)
+    taken[own] = True
+    c = cand[~taken[cand]]
+    _, first = np.unique(c, return_index=True)
+    c = c[np.sort(first)][: nsamples // 2]
+    taken[c] = True
+    parts = [c]
+    need = nsamples - len(c)
+    while need > 0:
+        draw = rng.integers(0, n, size=2 * need + 16)
+        draw = draw[~taken[draw]]
+        _, first = np.unique(draw, return_index=True)
+        draw = draw[np.sort(first)][:need]
+        taken[draw] = True
+        parts.append(draw)
+        need -= len(draw)
+    return np.concatenate(parts).astype(np.int64)
 
 
 def build_cds(X: np.ndarray, kernel: KernelSpec, leaf_size: int = 256, budget: float = 0.03,
@@ -594,7 +610,6 @@ def build_cds(X: np.ndarray, kernel: KernelSpec, leaf_size: int = 256, budget: f
     """Build the CDS of the kernel matrix of point set X (N x d, row-major)."""
     X = np.ascontiguousarray(X, dtype=np.float64)
     n = X.shape[0]
-    rng = np.random.default_rng(seed)
     tree = build_tree(X, leaf_size)
     near = near_lists(tree, budget)
     far = far_lists(tree, near)
@@ -624,33 +639,44 @@ def build_cds(X: np.ndarray, kernel: KernelSpec, leaf_size: int = 256, budget: f
     slen = np.zeros(nn, np.int32)
     skels: List[np.ndarray] = [np.zeros(0, np.int64)] * nn
     proj: List[np.ndarray] = [np.zeros((0, 0))] * nn
-    for lev in range(tree.depth, 0, -1):
-        for v in range((1 << lev) - 1, (1 << (lev + 1)) - 1):
-            own = tree.lids[v]
-            if lch[v] == -1:
-                bmap = own
-                cv = cand[v]
-            else:
-                l, r = int(lch[v]), int(rch[v])
-                bmap = np.concatenate([skels[l], skels[r]])
-                merged = np.concatenate([cand[l], cand[r]])
-                owns = np.zeros(n, bool)
-                owns[own] = True
-                merged = merged[~owns[merged]]
-                if merged.size:
-                    dist = sqdist(X[merged], X[bmap]).min(1)
-                    merged = merged[np.argsort(dist, kind="stable")]
-                    _, first = np.unique(merged, return_index=True)
-                    merged = merged[np.sort(first)]
-                cv = merged
-                cand[v] = merged[: 4 * leaf_size]
-            nsamples = max(2 * len(bmap), 2 * leaf_size)
-            amap = _sample_rows(X, own, cv, nsamples, n, rng)
-            K = kernel_matrix(X, amap, bmap, kernel)
-            piv, P = interpolative_decomposition(np.asfortranarray(K), tol, max_rank)
-            skels[v] = bmap[piv]
-            proj[v] = P
-            slen[v] = P.shape[0]
+
+    def compress(v: int):
+        own = tree.lids[v]
+        if lch[v] == -1:
+            bmap = own
+            cv = cand[v]
+            keep = None
+        else:
+            l, r = int(lch[v]), int(rch[v])
+            bmap = np.concatenate([skels[l], skels[r]])
+            merged = np.concatenate([cand[l], cand[r]])
+            owns = np.zeros(n, bool)
+            owns[own] = True
+            merged = merged[~owns[merged]]
+            if merged.size:
+                dist = sqdist(X[merged], X[bmap]).min(1)
+                merged = merged[np.argsort(dist, kind="stable")]
+                _, first = np.unique(merged, return_index=True)
+                merged = merged[np.sort(first)]
+            cv = merged
+            keep = merged[: 4 * leaf_size]
+        nsamples = max(2 * len(bmap), 2 * leaf_size)
+        amap = _sample_rows(own, cv, nsamples, n, np.random.default_rng([seed, v]))
+        K = kernel_matrix(X, amap, bmap, kernel)
+        piv, P = interpolative_decomposition(np.asfortranarray(K), tol, max_rank)
+        return v, bmap[piv], P, keep
+
+    # nodes of one level are independent: LAPACK / BLAS release the GIL, so a thread pool
+    # over the level with single-threaded BLAS inside scales with the host cores
+    with _blas_single_thread(), ThreadPoolExecutor(max_workers=_workers()) as pool:
+        for lev in range(tree.depth, 0, -1):
+            nodes = list(range((1 << lev) - 1, (1 << (lev + 1)) - 1))
+            for v, sk, P, keep in pool.map(compress, nodes):
+                skels[v] = sk
+                proj[v] = P
+                slen[v] = P.shape[0]
+                if keep is not None:
+                    cand[v] = keep
 
     # ---- pack (hcds.h) ----
     levelset, idx = levelsets_top_down(tree)
@@ -685,7 +711,8 @@ def build_cds(X: np.ndarray, kernel: KernelSpec, leaf_size: int = 256, budget: f
     Dsz = Ddim.astype(np.int64)[npx] * Ddim.astype(np.int64)[npy]
     Dptr = np.concatenate([[0], np.cumsum(Dsz)[:-1]]).astype(np.uint64)
     D = np.empty(int(Dsz.sum()))
-    for k in range(len(npx)):
+
+    def near_block(k):
         x, y = int(npx[k]), int(npy[k])
         blk = kernel_matrix(X, tree.lids[tree.leaf_node(x)], tree.lids[tree.leaf_node(y)], kernel)
         D[int(Dptr[k]):int(Dptr[k]) + blk.size] = blk.reshape(-1, order="F")
@@ -693,10 +720,15 @@ def build_cds(X: np.ndarray, kernel: KernelSpec, leaf_size: int = 256, budget: f
     Bsz = slen.astype(np.int64)[fpx] * slen.astype(np.int64)[fpy]
     Bptr = (np.concatenate([[0], np.cumsum(Bsz)[:-1]]) if len(fpx) else np.zeros(0)).astype(np.uint64)
     B = np.empty(int(Bsz.sum()))
-    for k in range(len(fpx)):
+
+    def far_block(k):
         x, y = int(fpx[k]), int(fpy[k])
         blk = kernel_matrix(X, skels[x], skels[y], kernel)
         B[int(Bptr[k]):int(Bptr[k]) + blk.size] = blk.reshape(-1, order="F")
+
+    with _blas_single_thread(), ThreadPoolExecutor(max_workers=_workers()) as pool:
+        list(pool.map(near_block, range(len(npx))))
+        list(pool.map(far_block, range(len(fpx))))
 
     perm = np.concatenate([tree.lids[tree.leaf_node(i)] for i in range(tree.nleaf)]).astype(np.int64)
     lofs = np.concatenate([[0], np.cumsum(Ddim.astype(np.int64))]).astype(np.int64)
