@@ -221,6 +221,26 @@ MXB_API int32_t mxb_plan_info(const mxb_plan *plan, uint64_t *device_bytes, int3
 MXB_API int32_t mxb_plan_read_workspaces(mxb_plan *plan, int32_t nrhs, const int32_t *wskeloffset,
                                  double *wskel, const int32_t *uskeloffset, double *uskel);
 
+/* ---- evaluation without device allocation ------------------------------------------------ */
+
+/* No counterpart in the reference (its evaluator runs on the host).  For callers that may
+ * not allocate device memory -- a framework whose pooling allocator owns the whole GPU, or a
+ * steady-state loop that must not call cudaMalloc / cudaFree because they can synchronise
+ * the device -- this computes dY (+)= K~ dW in FP64 like mxb_plan_evaluate and allocates
+ * nothing: `desc` carries HOST index arrays but DEVICE pointers in desc->D, desc->B and
+ * desc->VT (with their lengths); dW and dY are device arrays in the packed leaf-blocked
+ * layout.  Task lists, per-leaf offsets and skeleton workspaces live in one static device
+ * array of MXB_NOALLOC_SCRATCH_BYTES (32 MiB) that every GPU loading the library keeps until
+ * exit; larger problems (skeleton rows x nrhs x 16 bytes plus the task lists) are rejected
+ * with MXB_ERR_UNSUPPORTED.  The first call on a device looks the array's address up
+ * (cudaGetSymbolAddress), so make it before any stream capture.  Every call shares the
+ * array and overwrites all of it that it reads, so nothing needs clearing, but calls that
+ * overlap on the GPU (other streams, other host threads) race on it.  Asynchronous on
+ * `stream`. */
+#define MXB_NOALLOC_SCRATCH_BYTES (32u << 20)
+MXB_API int32_t mxb_evaluate_noalloc(const mxb_cds_desc *desc, const double *dW, double *dY, int32_t nrhs,
+                                     int32_t accumulate, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

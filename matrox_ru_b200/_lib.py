@@ -86,6 +86,7 @@ def load(path: str = LIB_PATH):
     lib.mxb_permute_rows.argtypes = [P, P, P, I32, I64, P, P, I64, I64, I32, I32, I32, P]
     lib.mxb_transform.argtypes = [P, P, P, I32, P, I64, I64, I32, P]
     lib.mxb_untransform.argtypes = [P, P, P, I32, P, I64, I64, I32, P]
+    lib.mxb_evaluate_noalloc.argtypes = [ctypes.POINTER(CdsDesc), P, P, I32, I32, P]
     lib.mxb_hgemm_set_shape.argtypes = [I32, I32, I32]
     lib.mxb_hgemm_hss_set_shape.argtypes = [I32, I32]
     cb = _REF_ARGS_H2B + [I32, I32, P, P, ctypes.c_int]
