@@ -216,6 +216,9 @@ MXB_API int32_t mxb_plan_flops(const mxb_plan *plan, int32_t nrhs, uint64_t *flo
 /* Bytes of CDS held on the device and number of kernel launches of one evaluation. */
 MXB_API int32_t mxb_plan_info(const mxb_plan *plan, uint64_t *device_bytes, int32_t *launches,
                       int32_t *precision);
+/* Waits for the device and reports a kernel-side failure of earlier evaluations on the plan
+ * (MXB_ERR_TIMEOUT when a bounded wait of a tensor-core kernel gave up); clears it. */
+MXB_API int32_t mxb_plan_status(mxb_plan *plan);
 /* Copies the last evaluation's skeleton workspaces (wskel, uskel) to host arrays laid out
  * with the caller's wskeloffset / uskeloffset (for callers that inspect them). */
 MXB_API int32_t mxb_plan_read_workspaces(mxb_plan *plan, int32_t nrhs, const int32_t *wskeloffset,

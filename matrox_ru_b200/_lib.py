@@ -83,6 +83,7 @@ def load(path: str = LIB_PATH):
     lib.mxb_plan_flops.argtypes = [P, I32, ctypes.POINTER(U64)]
     lib.mxb_plan_info.argtypes = [P, ctypes.POINTER(U64), ctypes.POINTER(I32), ctypes.POINTER(I32)]
     lib.mxb_plan_read_workspaces.argtypes = [P, I32, P, P, P, P]
+    lib.mxb_plan_status.argtypes = [P]
     lib.mxb_permute_rows.argtypes = [P, P, P, I32, I64, P, P, I64, I64, I32, I32, I32, P]
     lib.mxb_transform.argtypes = [P, P, P, I32, P, I64, I64, I32, P]
     lib.mxb_untransform.argtypes = [P, P, P, I32, P, I64, I64, I32, P]

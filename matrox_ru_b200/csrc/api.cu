@@ -764,9 +764,22 @@ int32_t mxb_plan_info(const mxb_plan *plan, uint64_t *device_bytes, int32_t *lau
     }
     const Plan *p = static_cast<const Plan *>(plan);
     if (device_bytes) *device_bytes = p->device_bytes;
-    if (launches) *launches = (int32_t)p->launches_fwd.size();
+    if (launches)
+        *launches = p->precision == MXB_PREC_SPLIT_BF16 ? (int32_t)split_bf16_launches(*p)
+                                                        : (int32_t)p->launches_fwd.size();
     if (precision) *precision = p->precision;
     return MXB_OK;
+}
+
+int32_t mxb_plan_status(mxb_plan *plan)
+{
+    if (!plan) {
+        set_error("null plan");
+        return MXB_ERR_ARG;
+    }
+    Plan *p = static_cast<Plan *>(plan);
+    API_CUDA(cudaDeviceSynchronize());
+    return split_bf16_status(*p);
 }
 
 int32_t mxb_plan_read_workspaces(mxb_plan *plan, int32_t nrhs, const int32_t *wskeloffset, double *wskel,

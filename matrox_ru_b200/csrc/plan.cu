@@ -45,6 +45,7 @@ int row_tile_for(int precision);
 
 Plan::~Plan()
 {
+    free_split_bf16();
     for (void *p : allocations) cudaFree(p);
 }
 

@@ -68,5 +68,7 @@ struct Plan : public mxb_plan {
 
 const char *last_error();
 int row_tile_for(int precision);
+int split_bf16_launches(const Plan &p);
+int split_bf16_status(Plan &p);
 
 }  // namespace mxb

@@ -1,23 +1,699 @@
-// Split-BF16 evaluation path (tcgen05 tensor cores).  Placeholder until the kernels land:
-// plans created with MXB_PREC_SPLIT_BF16 report MXB_ERR_UNSUPPORTED.
+// Split-BF16 evaluation path on the 5th-generation tensor cores (tcgen05).
+//
+// Precision scheme (per north-star: BF16 tensor-core products with split operands, FP32
+// accumulation, FP32-accurate transfers, FP64 final Y):
+//   near D_xy W_y and far B_xy wskel_y : both operands split into bf16 hi + mid, three
+//        products hi*hi + hi*mid + mid*hi ("bf16x3"), FP32 accumulation in TMEM.  Splitting
+//        only W leaves the CDS operand at 8 bits (~2e-3 relative error); splitting both
+//        gives ~5e-6.
+//   transfers (leaf / internal projections up and down): hi + mid + lo (24 bits), six
+//        products ("bf16x6"), which matches an FP32 SGEMM's error (~3e-7).
+//   Y: FP64, accumulated from the FP32 tile in the epilogue.
+//
+// Data layout: every operand lives in HBM already in the shared-memory tile format
+// (128 rows x 64 K bf16, K-major, 128-byte swizzle; parts of one tile contiguous), so each
+// pipeline stage is filled by a few 1-D bulk copies (cp.async.bulk) on an mbarrier -- no
+// tensor maps, no per-element address math in the main loop.  The CDS operands (D, B, the
+// projections and their transposes) are tiled once when the plan is created; W and the
+// skeleton vectors are tiled per evaluation by split kernels (HBM-bound passes).
+//
+// GEMM kernel: one CTA per (task row tile, 128|256 right-hand sides), 4 warps:
+//   warp 0 lane 0 : producer -- bulk copies of the A and B part tiles of each K step
+//   warp 1 lane 0 : MMA issuer -- tcgen05.mma M=128, N=BN, K=16, 3 or 6 per 16-K slice
+//   all 4 warps   : epilogue -- tcgen05.ld of the FP32 accumulator rows, coalesced stores
+// Every wait is bounded (tc::WAIT_CYCLES); a CTA that times out raises MXB_ERR_TIMEOUT in
+// the plan's error word, drains its own copies and MMAs, frees its TMEM and exits.
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "matrox_b200.h"
+#include "mxb_internal.h"
 #include "plan.h"
+#include "tc_common.cuh"
 
 namespace mxb {
 
 int row_tile_for(int precision) { return precision == MXB_PREC_SPLIT_BF16 ? 128 : 64; }
 
+namespace {
+
+using tc::TILE_BYTES;
+
+struct TcItem {
+    uint64_t a_off;   // byte offset of A's tile (0, 0) in the launch's A pool
+    int64_t b_base;   // K-tile base of the B operand's node / leaf in the B buffer
+    int32_t KT;       // K tiles of this item
+    int32_t pad;
+};
+
+struct SplitJob {     // one leaf block of W or one skeleton block -> tiled parts
+    int64_t src_row;  // leaf index (W) or skeleton row offset
+    int64_t dst_kt;   // K-tile base in the destination buffer
+    int32_t ld, K, KT, pad;
+};
+
+struct PoolJob {      // one CDS matrix -> tiled parts (plan creation)
+    uint64_t src_off;  // element offset in the FP64 pool
+    uint64_t dst_off;  // byte offset of tile (0, 0)
+    int32_t src_pool, ld, R, K, RT, KT, trans, parts;
+};
+
+struct TcArgs {
+    const uint8_t *a_pool;
+    const uint8_t *b_pool;
+    double *Y;
+    const int32_t *yofs;
+    float *skel;
+    int *err;
+    int NT;         // 128-column tiles per node in the B buffers (even)
+    int nrhs;
+    int out_kind;   // 0: FP64 Y, 1: FP32 skeleton block
+    int beta_arg;
+};
+
+// ---------------------------------------------------------------------------------------
+// tiling kernels
+// ---------------------------------------------------------------------------------------
+
+__device__ __forceinline__ void store_parts(uint8_t *tile0, int parts, int r, int c, const __nv_bfloat16 (&h)[8],
+                                            const __nv_bfloat16 (&m)[8], const __nv_bfloat16 (&l)[8])
+{
+    const uint32_t o = tc::swizzled_offset(r, c * 8);
+    uint4 vh, vm, vl;
+    memcpy(&vh, h, 16);
+    memcpy(&vm, m, 16);
+    memcpy(&vl, l, 16);
+    *reinterpret_cast<uint4 *>(tile0 + o) = vh;
+    *reinterpret_cast<uint4 *>(tile0 + TILE_BYTES + o) = vm;
+    if (parts > 2) *reinterpret_cast<uint4 *>(tile0 + 2 * TILE_BYTES + o) = vl;
+}
+
+// CDS matrix -> tiled parts.  op(A)(r, k) = trans ? src[k + r ld] : src[r + k ld].
+__global__ void __launch_bounds__(256) tile_pool_kernel(const PoolJob *__restrict__ jobs, const double *p0,
+                                                        const double *p1, const double *p2, uint8_t *dst)
+{
+    const PoolJob j = jobs[blockIdx.x];
+    const int kt = blockIdx.y, rt = blockIdx.z;
+    if (kt >= j.KT || rt >= j.RT) return;
+    const double *src = (j.src_pool == 0 ? p0 : (j.src_pool == 1 ? p1 : p2)) + j.src_off;
+    uint8_t *tile0 = dst + j.dst_off + ((size_t)rt * j.KT + kt) * (size_t)j.parts * TILE_BYTES;
+    for (int i = 0; i < 4; ++i) {
+        const int idx = threadIdx.x + i * 256;
+        const int r = j.trans ? idx / 8 : idx % 128;
+        const int c = j.trans ? idx % 8 : idx / 128;
+        const int gr = rt * 128 + r;
+        __nv_bfloat16 h[8], m[8], l[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            const int gk = kt * 64 + c * 8 + e;
+            double x = 0.0;
+            if (gr < j.R && gk < j.K) x = j.trans ? src[gk + (size_t)gr * j.ld] : src[gr + (size_t)gk * j.ld];
+            tc::split3(x, h[e], m[e], l[e]);
+        }
+        store_parts(tile0, j.parts, r, c, h, m, l);
+    }
+}
+
+// W (FP64, leaf-blocked) or a skeleton block (FP32) -> B-operand tiles with 3 parts.
+// B(n, k) = src[k + n ld]; rows n >= nrhs and k >= K are zero.
+template <typename T>
+__global__ void __launch_bounds__(256) split_b_kernel(const SplitJob *__restrict__ jobs, const T *__restrict__ base,
+                                                      const int32_t *__restrict__ ofs, int nrhs, int NT,
+                                                      uint8_t *__restrict__ dst)
+{
+    const SplitJob j = jobs[blockIdx.x];
+    const int kt = blockIdx.y, nt = blockIdx.z;
+    if (kt >= j.KT) return;
+    const T *src = base + (ofs ? (int64_t)ofs[j.src_row] : j.src_row * (int64_t)nrhs);
+    uint8_t *tile0 = dst + ((size_t)j.dst_kt * NT + (size_t)nt * j.KT + kt) * 3 * (size_t)TILE_BYTES;
+    for (int i = 0; i < 4; ++i) {
+        const int idx = threadIdx.x + i * 256;
+        const int c = idx % 8, r = idx / 8;
+        const int n = nt * 128 + r;
+        __nv_bfloat16 h[8], m[8], l[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            const int k = kt * 64 + c * 8 + e;
+            T x = T(0);
+            if (n < nrhs && k < j.K) x = src[k + (size_t)n * j.ld];
+            tc::split3(x, h[e], m[e], l[e]);
+        }
+        store_parts(tile0, 3, r, c, h, m, l);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// tcgen05 grouped GEMM
+// ---------------------------------------------------------------------------------------
+
+template <int P, int BN>
+struct TcCfg {
+    static constexpr int STAGES = 2;
+    static constexpr int HALVES = BN / 128;
+    static constexpr int A_BYTES = P * TILE_BYTES;
+    static constexpr int B_BYTES = HALVES * P * TILE_BYTES;
+    static constexpr int STAGE = A_BYTES + B_BYTES;
+    static constexpr int SMEM = STAGES * STAGE + 1024 + 256;
+    static constexpr int NPROD = P == 2 ? 3 : 6;
+};
+
+template <int P, int BN>
+__global__ void __launch_bounds__(128, 1)
+tc_gemm_kernel(const Task *__restrict__ tasks, const TcItem *__restrict__ items, TcArgs args)
+{
+    using C = TcCfg<P, BN>;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + C::STAGES * C::STAGE);
+    uint64_t *empty = full + C::STAGES;
+    uint64_t *accb = empty + C::STAGES;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(accb + 1);
+    volatile int *abort_word = reinterpret_cast<volatile int *>(tmem_slot + 1);
+
+    const Task t = tasks[blockIdx.x];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const TcItem *ti = items + t.item0;
+    int ktiles = 0;
+    for (int q = 0; q < t.nitem; ++q) ktiles += ti[q].KT;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < C::STAGES; ++s) {
+            tc::mbar_init(&full[s], 1);
+            tc::mbar_init(&empty[s], 1);
+        }
+        tc::mbar_init(accb, 1);
+        *abort_word = 0;
+        tc::fence_mbar_init();
+    }
+    if (warp == 0) tc::tmem_alloc(tmem_slot, BN);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0 && ktiles > 0) {
+        // ---------------- producer ----------------
+        int q = 0, kt = 0, issued = 0;
+        const int mt = t.m0 / 128;
+        for (int i = 0; i < ktiles; ++i) {
+            const int s = i % C::STAGES;
+            const uint32_t round = (uint32_t)(i / C::STAGES);
+            if (!tc::mbar_wait(&empty[s], (round & 1) ^ 1, abort_word)) {
+                *abort_word = 1;
+                break;
+            }
+            while (kt >= ti[q].KT) {
+                ++q;
+                kt = 0;
+            }
+            const TcItem it = ti[q];
+            uint8_t *sa = smem + s * C::STAGE;
+            uint8_t *sb = sa + C::A_BYTES;
+            tc::mbar_expect_tx(&full[s], C::STAGE);
+            const uint8_t *ga = args.a_pool + it.a_off + ((size_t)mt * it.KT + kt) * (size_t)P * TILE_BYTES;
+            tc::bulk_g2s(sa, ga, C::A_BYTES, &full[s]);
+#pragma unroll
+            for (int hh = 0; hh < C::HALVES; ++hh) {
+                const size_t nt = (size_t)blockIdx.y * C::HALVES + hh;
+                const uint8_t *gb = args.b_pool + ((size_t)it.b_base * args.NT + nt * it.KT + kt) * 3 * (size_t)TILE_BYTES;
+#pragma unroll
+                for (int p = 0; p < P; ++p)
+                    tc::bulk_g2s(sb + (p * C::HALVES + hh) * TILE_BYTES, gb + (size_t)p * TILE_BYTES, TILE_BYTES, &full[s]);
+            }
+            ++kt;
+            ++issued;
+        }
+        // drain: every stage this thread filled must have landed before the CTA may exit
+        for (int s = 0; s < C::STAGES && s < issued; ++s) {
+            const uint32_t last_round = (uint32_t)((issued - 1 - s) / C::STAGES);
+            volatile int never = 0;
+            tc::mbar_wait(&full[s], last_round & 1, &never);
+        }
+    } else if (warp == 1 && lane == 0 && ktiles > 0) {
+        // ---------------- MMA issuer ----------------
+        constexpr uint32_t IDESC = tc::idesc_bf16_f32(128, BN);
+        constexpr int PA[6] = {0, 0, 1, 0, 1, 2};
+        constexpr int PB[6] = {0, 1, 0, 2, 1, 0};
+        uint32_t acc = 0;
+        for (int i = 0; i < ktiles; ++i) {
+            const int s = i % C::STAGES;
+            const uint32_t round = (uint32_t)(i / C::STAGES);
+            if (!tc::mbar_wait(&full[s], round & 1, abort_word)) {
+                *abort_word = 1;
+                break;
+            }
+            tc::fence_after_sync();
+            const uint32_t sa = tc::smem_u32(smem + s * C::STAGE);
+            const uint32_t sb = sa + C::A_BYTES;
+#pragma unroll
+            for (int ks = 0; ks < 4; ++ks) {
+#pragma unroll
+                for (int j = 0; j < C::NPROD; ++j) {
+                    const uint64_t ad = tc::smem_desc_sw128(sa + PA[j] * TILE_BYTES + ks * 32);
+                    const uint64_t bd = tc::smem_desc_sw128(sb + PB[j] * C::HALVES * TILE_BYTES + ks * 32);
+                    tc::mma_bf16(tmem, ad, bd, IDESC, acc);
+                    acc = 1;
+                }
+            }
+            tc::mma_commit(&empty[s]);
+        }
+        tc::mma_commit(accb);  // arrives once every MMA issued above has completed
+    }
+    __syncwarp();
+
+    // ---------------- epilogue ----------------
+    if (ktiles > 0) {
+        volatile int never = 0;  // a timed-out CTA still waits (bounded) for its MMAs
+        if (!tc::mbar_wait(accb, 0, &never)) *abort_word = 1;
+    }
+    __syncthreads();  // makes `aborted` (and so the tcgen05.ld below) uniform across the CTA
+    tc::fence_after_sync();
+    const bool aborted = *abort_word != 0;
+    const bool have = ktiles > 0 && !aborted;
+    if (aborted && threadIdx.x == 0) atomicExch(args.err, MXB_ERR_TIMEOUT);
+    const int r = t.m0 + warp * 32 + lane;
+    const bool row_ok = r < t.M && !aborted;
+    const int beta = t.beta == 2 ? args.beta_arg : t.beta;
+    const int col0 = blockIdx.y * BN;
+#pragma unroll 1
+    for (int c0 = 0; c0 < BN; c0 += 32) {
+        float v[32];
+        if (have) {
+            tc::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+        } else {
+#pragma unroll
+            for (int e = 0; e < 32; ++e) v[e] = 0.f;
+        }
+        if (!row_ok) continue;
+        if (args.out_kind == 0) {
+            double *Yb = args.Y + args.yofs[t.c_row] + r;
+#pragma unroll
+            for (int e = 0; e < 32; ++e) {
+                const int col = col0 + c0 + e;
+                if (col < args.nrhs) {
+                    double *p = Yb + (size_t)col * t.ldc;
+                    *p = beta ? *p + (double)v[e] : (double)v[e];
+                }
+            }
+        } else {
+            float *Sb = args.skel + t.c_row * (int64_t)args.nrhs + r;
+#pragma unroll
+            for (int e = 0; e < 32; ++e) {
+                const int col = col0 + c0 + e;
+                if (col < args.nrhs) {
+                    float *p = Sb + (size_t)col * t.ldc;
+                    *p = beta ? *p + v[e] : v[e];
+                }
+            }
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, BN);
+}
+
+template <int P, int BN>
+cudaError_t launch_tc(const Task *tasks, const TcItem *items, int ntasks, const TcArgs &a, cudaStream_t s)
+{
+    if (ntasks <= 0) return cudaSuccess;
+    using C = TcCfg<P, BN>;
+    cudaError_t e = cudaFuncSetAttribute(tc_gemm_kernel<P, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
+    if (e != cudaSuccess) return e;
+    dim3 grid(ntasks, (a.nrhs + BN - 1) / BN);
+    tc_gemm_kernel<P, BN><<<grid, 128, C::SMEM, s>>>(tasks, items, a);
+    return cudaGetLastError();
+}
+
+enum OpKind { OP_SPLIT_W, OP_SPLIT_WSKEL, OP_SPLIT_USKEL, OP_TC2, OP_TC3 };
+enum APool { POOL_D2, POOL_F2, POOL_VU3, POOL_VD3, NPOOL };
+enum BBuf { BUF_W, BUF_WSKEL, BUF_USKEL };
+
+struct Op {
+    int kind, first, count, max_kt;
+    int a_pool, b_buf, out_kind;
+};
+
+int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+}  // namespace
+
+struct SplitBF16 {
+    uint8_t *pool[NPOOL] = {};
+    size_t pool_bytes[NPOOL] = {};
+    Task *dTasks = nullptr;
+    TcItem *dItems = nullptr;
+    SplitJob *dJobs = nullptr;
+    int *dErr = nullptr;
+    std::vector<Op> ops;
+    std::vector<Task> tasks;
+    std::vector<TcItem> items;
+    std::vector<SplitJob> jobs;
+    std::vector<int64_t> leaf_kt, node_kt;  // K-tile bases
+    int64_t leaf_kt_total = 0, node_kt_total = 0;
+    int nt_cap = 0, nrhs_cap = 0;
+    uint8_t *Wt = nullptr, *wT = nullptr, *uT = nullptr;
+    float *w32 = nullptr, *u32 = nullptr;
+};
+
 int Plan::setup_split_bf16(const mxb_cds_desc &)
 {
-    set_error("split-BF16 path not built yet");
-    return MXB_ERR_UNSUPPORTED;
+    SplitBF16 *S = new SplitBF16();
+    bf16 = S;
+    auto KT = [](int64_t k) { return (int32_t)ceil_div(std::max<int64_t>(k, 0), 64); };
+    auto RT = [](int64_t r) { return (int32_t)ceil_div(std::max<int64_t>(r, 0), 128); };
+    auto projects = [&](int v) { return v != root && slen[v] > 0; };
+
+    // ---- K-tile bases of the B operands (per-evaluation buffers) ----
+    S->leaf_kt.resize(nleaf);
+    for (int i = 0; i < nleaf; ++i) {
+        S->leaf_kt[i] = S->leaf_kt_total;
+        S->leaf_kt_total += KT(Ddim[i]);
+    }
+    S->node_kt.assign(numnodes, 0);
+    for (int v : bfs) {
+        S->node_kt[v] = S->node_kt_total;
+        S->node_kt_total += KT(slen[v]);
+    }
+
+    // ---- CDS pools: tiling jobs ----
+    std::vector<PoolJob> pj[NPOOL];
+    auto add_pool = [&](int pool, int src_pool, uint64_t src_off, int ld, int R, int K, int trans, int parts) {
+        PoolJob j{};
+        j.src_pool = src_pool;
+        j.src_off = src_off;
+        j.ld = ld;
+        j.R = R;
+        j.K = K;
+        j.RT = RT(R);
+        j.KT = KT(K);
+        j.trans = trans;
+        j.parts = parts;
+        j.dst_off = S->pool_bytes[pool];
+        S->pool_bytes[pool] += (size_t)j.RT * j.KT * parts * TILE_BYTES;
+        pj[pool].push_back(j);
+        return j.dst_off;
+    };
+    std::vector<uint64_t> near_a(near_x.size()), far_a(far_x.size());
+    for (size_t k = 0; k < near_x.size(); ++k)
+        near_a[k] = add_pool(POOL_D2, 0, near_off[k], Ddim[near_x[k]], Ddim[near_x[k]], Ddim[near_y[k]], 0, 2);
+    for (size_t k = 0; k < far_x.size(); ++k)
+        far_a[k] = add_pool(POOL_F2, 1, far_off[k], slen[far_x[k]], slen[far_x[k]], slen[far_y[k]], 0, 2);
+    std::vector<uint64_t> up_a(numnodes), up_b(numnodes), down_a(numnodes);
+    for (int v = 0; v < numnodes; ++v) {
+        if (!projects(v)) continue;
+        const int s = slen[v];
+        if (lch[v] == -1) {
+            up_a[v] = add_pool(POOL_VU3, 2, (uint64_t)VTptr[v], s, s, Ddim[lm[v]], 0, 3);
+            down_a[v] = add_pool(POOL_VD3, 2, (uint64_t)VTptr[v], s, Ddim[lm[v]], s, 1, 3);  // leaf down: P_v^T
+        } else {
+            const int l = lch[v], r = rch[v];
+            up_a[v] = add_pool(POOL_VU3, 2, (uint64_t)VTptr[v], s, s, slen[l], 0, 3);
+            up_b[v] = add_pool(POOL_VU3, 2, (uint64_t)VTptr[v] + (uint64_t)s * slen[l], s, s, slen[r], 0, 3);
+        }
+    }
+    // down slices: child c of projecting parent p: op(A) = P_p[:, part of c]^T (s_c x s_p)
+    std::vector<uint64_t> down_child(numnodes);
+    for (int c = 0; c < numnodes; ++c) {
+        const int p = parent[c];
+        if (p < 0 || !projects(p) || !projects(c)) continue;
+        const uint64_t off = (uint64_t)VTptr[p] + (c == rch[p] ? (uint64_t)slen[p] * slen[lch[p]] : 0);
+        down_child[c] = add_pool(POOL_VD3, 2, off, slen[p], slen[c], slen[p], 1, 3);
+    }
+    for (int pidx = 0; pidx < NPOOL; ++pidx) {
+        int rc = alloc((void **)&S->pool[pidx], std::max<size_t>(S->pool_bytes[pidx], 16));
+        if (rc) return rc;
+        if (pj[pidx].empty()) continue;
+        PoolJob *dj = nullptr;
+        rc = alloc((void **)&dj, pj[pidx].size() * sizeof(PoolJob));
+        if (rc) return rc;
+        cudaError_t e = cudaMemcpy(dj, pj[pidx].data(), pj[pidx].size() * sizeof(PoolJob), cudaMemcpyHostToDevice);
+        int maxkt = 1, maxrt = 1;
+        for (auto &j : pj[pidx]) {
+            maxkt = std::max(maxkt, j.KT);
+            maxrt = std::max(maxrt, j.RT);
+        }
+        if (e == cudaSuccess) {
+            tile_pool_kernel<<<dim3((unsigned)pj[pidx].size(), maxkt, maxrt), 256>>>(dj, dD, dB, dVT, S->pool[pidx]);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) {
+            set_error(std::string("tiling the CDS for the split-BF16 path: ") + cudaGetErrorString(e));
+            return MXB_ERR_CUDA;
+        }
+    }
+
+    // ---- task lists and op sequence (forward) ----
+    int maxh = 0, maxd = 0;
+    for (int v = 0; v < numnodes; ++v) {
+        maxh = std::max(maxh, height[v]);
+        maxd = std::max(maxd, depth[v]);
+    }
+    auto begin_op = [&](int kind, int a_pool, int b_buf, int out_kind) {
+        Op o{};
+        o.kind = kind;
+        o.a_pool = a_pool;
+        o.b_buf = b_buf;
+        o.out_kind = out_kind;
+        o.first = (kind <= OP_SPLIT_USKEL) ? (int)S->jobs.size() : (int)S->tasks.size();
+        S->ops.push_back(o);
+    };
+    auto end_op = [&]() {
+        Op &o = S->ops.back();
+        o.count = ((o.kind <= OP_SPLIT_USKEL) ? (int)S->jobs.size() : (int)S->tasks.size()) - o.first;
+        o.max_kt = 1;
+        if (o.kind <= OP_SPLIT_USKEL)
+            for (int j = o.first; j < o.first + o.count; ++j) o.max_kt = std::max(o.max_kt, S->jobs[j].KT);
+        if (o.count == 0) S->ops.pop_back();
+    };
+    auto add_tasks = [&](int16_t c_kind, int64_t c_row, int ldc, int M, int item0, int16_t beta) {
+        for (int m0 = 0; m0 < M; m0 += 128) {
+            Task t{};
+            t.c_row = c_row;
+            t.ldc = ldc;
+            t.M = M;
+            t.m0 = m0;
+            t.item0 = item0;
+            t.nitem = (int)S->items.size() - item0;
+            t.c_kind = c_kind;
+            t.beta = beta;
+            S->tasks.push_back(t);
+        }
+    };
+    auto item = [&](uint64_t a_off, int64_t b_base, int K) {
+        TcItem it{};
+        it.a_off = a_off;
+        it.b_base = b_base;
+        it.KT = KT(K);
+        if (it.KT > 0) S->items.push_back(it);
+    };
+    auto split_job = [&](int64_t src_row, int64_t dst_kt, int ld, int K) {
+        SplitJob j{};
+        j.src_row = src_row;
+        j.dst_kt = dst_kt;
+        j.ld = ld;
+        j.K = K;
+        j.KT = KT(K);
+        if (j.KT > 0) S->jobs.push_back(j);
+    };
+
+    // W -> tiles
+    begin_op(OP_SPLIT_W, -1, BUF_W, -1);
+    for (int i = 0; i < nleaf; ++i) split_job(i, S->leaf_kt[i], Ddim[i], Ddim[i]);
+    end_op();
+    // up-sweep by height
+    for (int h = 0; h <= maxh; ++h) {
+        begin_op(OP_TC3, POOL_VU3, h == 0 ? BUF_W : BUF_WSKEL, 1);
+        for (int v : bfs) {
+            if (height[v] != h || !projects(v)) continue;
+            const int item0 = (int)S->items.size();
+            if (lch[v] == -1) {
+                item(up_a[v], S->leaf_kt[lm[v]], Ddim[lm[v]]);
+            } else {
+                if (slen[lch[v]] > 0) item(up_a[v], S->node_kt[lch[v]], slen[lch[v]]);
+                if (slen[rch[v]] > 0) item(up_b[v], S->node_kt[rch[v]], slen[rch[v]]);
+            }
+            add_tasks(KIND_WSKEL, skel_row[v], slen[v], slen[v], item0, 0);
+        }
+        end_op();
+        begin_op(OP_SPLIT_WSKEL, -1, BUF_WSKEL, -1);
+        for (int v : bfs)
+            if (height[v] == h && projects(v)) split_job(skel_row[v], S->node_kt[v], slen[v], slen[v]);
+        end_op();
+    }
+    // far + down by depth
+    std::vector<std::vector<int>> far_out(numnodes);
+    for (size_t k = 0; k < far_x.size(); ++k) far_out[far_x[k]].push_back((int)k);
+    for (int dd = 1; dd <= maxd; ++dd) {
+        begin_op(OP_TC2, POOL_F2, BUF_WSKEL, 1);
+        for (int c : bfs) {
+            if (depth[c] != dd || !projects(c)) continue;
+            const int item0 = (int)S->items.size();
+            for (int k : far_out[c])
+                if (slen[far_y[k]] > 0) item(far_a[k], S->node_kt[far_y[k]], slen[far_y[k]]);
+            add_tasks(KIND_USKEL, skel_row[c], slen[c], slen[c], item0, 0);
+        }
+        end_op();
+        begin_op(OP_TC3, POOL_VD3, BUF_USKEL, 1);
+        for (int c : bfs) {
+            if (depth[c] != dd || !projects(c)) continue;
+            const int p = parent[c];
+            if (p < 0 || !projects(p)) continue;
+            const int item0 = (int)S->items.size();
+            item(down_child[c], S->node_kt[p], slen[p]);
+            add_tasks(KIND_USKEL, skel_row[c], slen[c], slen[c], item0, 1);
+        }
+        end_op();
+        begin_op(OP_SPLIT_USKEL, -1, BUF_USKEL, -1);
+        for (int c : bfs)
+            if (depth[c] == dd && projects(c) && lch[c] != -1) split_job(skel_row[c], S->node_kt[c], slen[c], slen[c]);
+        for (int c : bfs)  // leaves' uskel feeds the leaf-down launch
+            if (depth[c] == dd && projects(c) && lch[c] == -1) split_job(skel_row[c], S->node_kt[c], slen[c], slen[c]);
+        end_op();
+    }
+    // near (Y (+)= D W) then leaf down (Y += P^T uskel)
+    std::vector<std::vector<int>> near_out(nleaf);
+    for (size_t k = 0; k < near_x.size(); ++k) near_out[near_x[k]].push_back((int)k);
+    begin_op(OP_TC2, POOL_D2, BUF_W, 0);
+    for (int v : bfs) {
+        if (lch[v] != -1) continue;
+        const int x = lm[v];
+        const int item0 = (int)S->items.size();
+        for (int k : near_out[x]) item(near_a[k], S->leaf_kt[near_y[k]], Ddim[near_y[k]]);
+        add_tasks(KIND_Y, x, Ddim[x], Ddim[x], item0, 2);
+    }
+    end_op();
+    begin_op(OP_TC3, POOL_VD3, BUF_USKEL, 0);
+    for (int v : bfs) {
+        if (lch[v] != -1 || !projects(v)) continue;
+        const int item0 = (int)S->items.size();
+        item(down_a[v], S->node_kt[v], slen[v]);
+        add_tasks(KIND_Y, lm[v], Ddim[lm[v]], Ddim[lm[v]], item0, 1);
+    }
+    end_op();
+
+    int rc = alloc((void **)&S->dTasks, std::max<size_t>(S->tasks.size(), 1) * sizeof(Task));
+    if (!rc) rc = alloc((void **)&S->dItems, std::max<size_t>(S->items.size(), 1) * sizeof(TcItem));
+    if (!rc) rc = alloc((void **)&S->dJobs, std::max<size_t>(S->jobs.size(), 1) * sizeof(SplitJob));
+    if (!rc) rc = alloc((void **)&S->dErr, sizeof(int));
+    if (rc) return rc;
+    cudaError_t e = cudaMemcpy(S->dTasks, S->tasks.data(), S->tasks.size() * sizeof(Task), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !S->items.empty())
+        e = cudaMemcpy(S->dItems, S->items.data(), S->items.size() * sizeof(TcItem), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !S->jobs.empty())
+        e = cudaMemcpy(S->dJobs, S->jobs.data(), S->jobs.size() * sizeof(SplitJob), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(S->dErr, 0, sizeof(int));
+    if (e != cudaSuccess) {
+        set_error(std::string("uploading split-BF16 task lists: ") + cudaGetErrorString(e));
+        return MXB_ERR_CUDA;
+    }
+    return MXB_OK;
 }
 
-int Plan::run_split_bf16(const std::vector<Launch> &, const double *, double *, int, int, cudaStream_t)
+static int split_buffers(Plan &p, SplitBF16 &S, int nrhs)
 {
-    set_error("split-BF16 path not built yet");
-    return MXB_ERR_UNSUPPORTED;
+    const int NT = 2 * (int)ceil_div(nrhs, 256);  // even: BN = 256 launches read tile pairs
+    if (NT <= S.nt_cap && nrhs <= S.nrhs_cap) return MXB_OK;
+    auto release = [&](void *q) {
+        if (!q) return;
+        cudaFree(q);
+        p.allocations.erase(std::remove(p.allocations.begin(), p.allocations.end(), q), p.allocations.end());
+    };
+    release(S.Wt);
+    release(S.wT);
+    release(S.uT);
+    release(S.w32);
+    release(S.u32);
+    S.Wt = S.wT = S.uT = nullptr;
+    S.w32 = S.u32 = nullptr;
+    const size_t tile3 = 3 * (size_t)TILE_BYTES;
+    int rc = p.alloc((void **)&S.Wt, std::max<int64_t>(S.leaf_kt_total, 1) * NT * tile3);
+    if (!rc) rc = p.alloc((void **)&S.wT, std::max<int64_t>(S.node_kt_total, 1) * NT * tile3);
+    if (!rc) rc = p.alloc((void **)&S.uT, std::max<int64_t>(S.node_kt_total, 1) * NT * tile3);
+    if (!rc) rc = p.alloc((void **)&S.w32, std::max<int64_t>(p.skel_total, 1) * (size_t)nrhs * sizeof(float));
+    if (!rc) rc = p.alloc((void **)&S.u32, std::max<int64_t>(p.skel_total, 1) * (size_t)nrhs * sizeof(float));
+    if (rc) return rc;
+    S.nt_cap = NT;
+    S.nrhs_cap = nrhs;
+    return MXB_OK;
 }
 
-void Plan::free_split_bf16() {}
+int Plan::run_split_bf16(const std::vector<Launch> &L, const double *dW, double *dY, int nrhs, int accumulate,
+                         cudaStream_t stream)
+{
+    if (&L == &launches_adj) {
+        set_error("the adjoint runs in FP64 mode only (create an FP64 plan for mxb_plan_adjoint)");
+        return MXB_ERR_UNSUPPORTED;
+    }
+    SplitBF16 &S = *bf16;
+    int rc = split_buffers(*this, S, nrhs);
+    if (rc) return rc;
+    const int NT = S.nt_cap;
+    cudaError_t e = cudaSuccess;
+    for (const Op &o : S.ops) {
+        switch (o.kind) {
+        case OP_SPLIT_W:
+            split_b_kernel<double><<<dim3(o.count, o.max_kt, NT), 256, 0, stream>>>(S.dJobs + o.first, dW, dOfs,
+                                                                                  nrhs, NT, S.Wt);
+            break;
+        case OP_SPLIT_WSKEL:
+        case OP_SPLIT_USKEL:
+            split_b_kernel<float><<<dim3(o.count, o.max_kt, NT), 256, 0, stream>>>(
+                S.dJobs + o.first, o.kind == OP_SPLIT_WSKEL ? S.w32 : S.u32, nullptr, nrhs, NT,
+                o.kind == OP_SPLIT_WSKEL ? S.wT : S.uT);
+            break;
+        default: {
+            TcArgs a{};
+            a.a_pool = S.pool[o.a_pool];
+            a.b_pool = o.b_buf == BUF_W ? S.Wt : (o.b_buf == BUF_WSKEL ? S.wT : S.uT);
+            a.Y = dY;
+            a.yofs = dOfs + nleaf;
+            a.err = S.dErr;
+            a.NT = NT;
+            a.nrhs = nrhs;
+            a.out_kind = o.out_kind == 0 ? 0 : 1;
+            // skeleton outputs: far/down write uskel, the up-sweep writes wskel
+            a.skel = (o.a_pool == POOL_VU3) ? S.w32 : S.u32;
+            a.beta_arg = accumulate ? 1 : 0;
+            if (o.kind == OP_TC2) e = launch_tc<2, 256>(S.dTasks + o.first, S.dItems, o.count, a, stream);
+            else e = launch_tc<3, 128>(S.dTasks + o.first, S.dItems, o.count, a, stream);
+            break;
+        }
+        }
+        if (e == cudaSuccess) e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            set_error(std::string("split-BF16 launch: ") + cudaGetErrorString(e));
+            return MXB_ERR_CUDA;
+        }
+    }
+    return MXB_OK;
+}
+
+int split_bf16_launches(const Plan &p) { return p.bf16 ? (int)p.bf16->ops.size() : 0; }
+
+int split_bf16_status(Plan &p)
+{
+    if (!p.bf16) return MXB_OK;
+    int h = 0;
+    cudaError_t e = cudaMemcpy(&h, p.bf16->dErr, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+        set_error(std::string("reading the error word: ") + cudaGetErrorString(e));
+        return MXB_ERR_CUDA;
+    }
+    if (h) {
+        cudaMemset(p.bf16->dErr, 0, sizeof(int));
+        set_error("a tensor-core kernel wait timed out (MXB_ERR_TIMEOUT)");
+        return h;
+    }
+    return MXB_OK;
+}
+
+void Plan::free_split_bf16()
+{
+    delete bf16;
+    bf16 = nullptr;
+}
 
 }  // namespace mxb

@@ -230,6 +230,10 @@ class Plan:
         check(_lib.load().mxb_plan_info(self._h, ctypes.byref(b), ctypes.byref(l), ctypes.byref(p)), "mxb_plan_info")
         return {"device_bytes": int(b.value), "launches": int(l.value), "precision": int(p.value)}
 
+    def status(self) -> None:
+        """Synchronise and raise if a kernel of an earlier evaluation reported a failure."""
+        check(_lib.load().mxb_plan_status(self._h), "mxb_plan_status")
+
     def _check_operand(self, t, nrhs):
         torch = _torch()
         if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):

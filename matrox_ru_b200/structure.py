@@ -522,6 +522,21 @@ class CDS:
         f += int((2 * sl[self.fpairx] * sl[self.fpairy] * nrhs).sum())
         return f
 
+    def flops_breakdown(self, nrhs: int) -> Dict[str, int]:
+        """Algorithmic flops per pass: tree (up + down projections), near, far."""
+        tree = 0
+        for v in range(1, self.numnodes):
+            s = int(self.slen[v])
+            if self.lchildren[v] == -1:
+                tree += 2 * s * nrhs * int(self.Ddim[self.lm[v]])
+            else:
+                tree += 2 * s * (int(self.slen[self.lchildren[v]]) + int(self.slen[self.rchildren[v]])) * nrhs
+        dd = self.Ddim.astype(np.int64)
+        sl = self.slen.astype(np.int64)
+        return {"tree": 2 * tree,
+                "near": int((2 * dd[self.npairx] * dd[self.npairy] * nrhs).sum()),
+                "far": int((2 * sl[self.fpairx] * sl[self.fpairy] * nrhs).sum())}
+
     def to_tree_order(self, W: np.ndarray) -> np.ndarray:
         """``transform`` (``hcds.h:766-788``): W (N x r, column-major) -> TW with each
         leaf's rows contiguous per column block (leaf-blocked, tree order)."""
