@@ -37,7 +37,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--precision", choices=["fp64", "split_bf16", "both"], default="both")
+    ap.add_argument("--precision", choices=["fp64", "split_bf16", "split_bf16_far6", "split_bf16_x6", "all"],
+                    default="all")
     ap.add_argument("--n", type=int, default=None, help="override N (small smoke runs only)")
     ap.add_argument("--nrhs", type=int, default=None)
     ap.add_argument("--no-e2e", action="store_true")
@@ -230,16 +231,19 @@ def main():
     r = cfg["nrhs"]
     flops = cds.flops(r)
     fb = cds.flops_breakdown(r)
-    # tensor-core flops the split path executes: 3 bf16 products for near / far, 6 for the
-    # FP32-accurate transfers
-    exec_split = 3 * (fb["near"] + fb["far"]) + 6 * fb["tree"]
+    # tensor-core flops each split mode executes: 3 or 6 bf16 products per algorithmic product
+    exec_flops = {"fp64": flops,
+                  "split_bf16": 3 * (fb["near"] + fb["far"]) + 6 * fb["tree"],
+                  "split_bf16_far6": 3 * fb["near"] + 6 * (fb["far"] + fb["tree"]),
+                  "split_bf16_x6": 6 * flops}
     gen = torch.Generator(device=dev)
     gen.manual_seed(cfg["seed"] + 1 + rank)
     TW = torch.randn(cds.n * r, dtype=torch.float64, device=dev, generator=gen)
     peaks, peak_src = measured_peaks()
     fp64_peak = fp64_peak_tflops(torch, dev)
 
-    modes = ["fp64", "split_bf16"] if args.precision == "both" else [args.precision]
+    modes = ["fp64", "split_bf16", "split_bf16_far6", "split_bf16_x6"] if args.precision == "all" \
+        else [args.precision]
     results = {}
     clocks = None
     stream = torch.cuda.current_stream()
@@ -276,7 +280,7 @@ def main():
             ms = float(t.item())
         info = plan.info()
         res = {"ms": round(ms, 4),
-               "executed_tflops": round((exec_split if mode == "split_bf16" else flops) / (ms * 1e-3) / 1e12, 2), "gflops": round(flops / (ms * 1e-3) / 1e9, 1), "launches_per_eval": info["launches"],
+               "executed_tflops": round(exec_flops[mode] / (ms * 1e-3) / 1e12, 2), "gflops": round(flops / (ms * 1e-3) / 1e9, 1), "launches_per_eval": info["launches"],
                "device_bytes": info["device_bytes"], "step_ms_min": round(min(per), 4),
                "step_ms_max": round(max(per), 4), "clocks": cs.summary()}
         # accuracy on this CDS: vs the reference's FP64 evaluation (16-column slice) and vs dense
@@ -304,6 +308,8 @@ def main():
 
     ok = {m: v for m, v in results.items() if "ms" in v and
           (m == "fp64" or v.get("rel_err_vs_reference_same_cds", 1.0) <= 1e-5)}
+    if not ok:  # a single split mode was requested and missed the accuracy bar: report it anyway
+        ok = {m: v for m, v in results.items() if "ms" in v}
     best = min(ok, key=lambda m: ok[m]["ms"])
     head = ok[best]
     ms = head["ms"]
@@ -316,12 +322,12 @@ def main():
                 "kernel": "gemm_f64_kernel (all launches of one evaluation)",
                 "per_launch_flops": flops // max(head["launches_per_eval"], 1)}
     else:
-        roof = {"bound": "tensor", "achieved": round(exec_split / (ms * 1e-3) / 1e12, 3),
+        roof = {"bound": "tensor", "achieved": round(exec_flops[best] / (ms * 1e-3) / 1e12, 3),
                 "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
                 "peak_source": f"MEASURED_PEAKS.json bf16_tflops ({peak_src}, burst)",
                 "kernel": "tc_gemm_kernel + split kernels (all launches of one evaluation)",
-                "flops_counted": "executed bf16 tensor flops: 3x(near+far) + 6x(transfers)",
-                "per_launch_flops": exec_split // max(head["launches_per_eval"], 1)}
+                "flops_counted": "executed bf16 tensor flops (3 or 6 products per algorithmic product)",
+                "per_launch_flops": exec_flops[best] // max(head["launches_per_eval"], 1)}
     roof["frac"] = round(roof["achieved"] / roof["peak"], 4)
     roof["traffic"] = traffic
 
@@ -379,7 +385,9 @@ def main():
     line = {
         "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if best == "fp64" else "bf16x3(split)+f32+f64", "data": "synthetic",
+        "dtype": {"fp64": "f64", "split_bf16": "bf16x3 near/far, bf16x6 transfers, f32 acc, f64 Y",
+                  "split_bf16_far6": "bf16x3 near, bf16x6 far/transfers, f32 acc, f64 Y",
+                  "split_bf16_x6": "bf16x6, f32 acc, f64 Y"}[best], "data": "synthetic",
         "config": dict(cfg, precision=best, flops_per_eval=flops, flops_breakdown=fb,
                        inputs="larger than L2: W 512 MiB and CDS > 2 GiB read every step",
                        parallelism=f"replicas x{world} (weak scaling; no data-path collective)"),

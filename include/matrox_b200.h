@@ -48,8 +48,12 @@ extern "C" {
 
 /* ---- precision modes --------------------------------------------------------------- */
 #define MXB_PREC_FP64 0       /* FP64 everywhere (reference mode)                        */
-#define MXB_PREC_SPLIT_BF16 1 /* near/far on BF16 tensor cores with hi+lo split operands,
-                                 FP32 accumulation; transfers FP32; FP64 final Y        */
+#define MXB_PREC_SPLIT_BF16 1 /* tensor cores (tcgen05, BF16 in, FP32 accumulate), both
+                                 operands split: near and far couplings hi+mid with 3
+                                 products, transfers hi+mid+lo with 6 products (FP32
+                                 accuracy); FP64 final Y                                  */
+#define MXB_PREC_SPLIT_BF16_FAR6 2 /* as MXB_PREC_SPLIT_BF16 with 6-product far couplings */
+#define MXB_PREC_SPLIT_BF16_X6 3   /* 6 products (hi+mid+lo) for every GEMM               */
 
 /* ---- flags for the drop-ins ---------------------------------------------------------- */
 #define MXB_FLAG_MIRROR_WORKSPACES 1u /* copy wskel/uskel back to the caller's arrays    */

@@ -21,6 +21,8 @@ MXB_ERR_TIMEOUT = -5
 MXB_ERR_UNSUPPORTED = -6
 PREC_FP64 = 0
 PREC_SPLIT_BF16 = 1
+PREC_SPLIT_BF16_FAR6 = 2
+PREC_SPLIT_BF16_X6 = 3
 FLAG_MIRROR_WORKSPACES = 1
 FLAG_OUTPUT_IS_ZERO = 2
 

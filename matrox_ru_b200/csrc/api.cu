@@ -425,7 +425,7 @@ const char *mxb_version(void) { return "matrox_b200 0.1 (sm_100a)"; }
 
 int32_t mxb_set_precision(int32_t mode)
 {
-    if (mode != MXB_PREC_FP64 && mode != MXB_PREC_SPLIT_BF16) {
+    if (mode < MXB_PREC_FP64 || mode > MXB_PREC_SPLIT_BF16_X6) {
         set_error("unknown precision mode");
         return MXB_ERR_ARG;
     }
@@ -765,7 +765,7 @@ int32_t mxb_plan_info(const mxb_plan *plan, uint64_t *device_bytes, int32_t *lau
     const Plan *p = static_cast<const Plan *>(plan);
     if (device_bytes) *device_bytes = p->device_bytes;
     if (launches)
-        *launches = p->precision == MXB_PREC_SPLIT_BF16 ? (int32_t)split_bf16_launches(*p)
+        *launches = p->precision != MXB_PREC_FP64 ? (int32_t)split_bf16_launches(*p)
                                                         : (int32_t)p->launches_fwd.size();
     if (precision) *precision = p->precision;
     return MXB_OK;

@@ -369,7 +369,7 @@ uint64_t Plan::flops(int nrhs) const
 
 int Plan::create(const mxb_cds_desc &d, int prec, Plan **out)
 {
-    if (prec != MXB_PREC_FP64 && prec != MXB_PREC_SPLIT_BF16) {
+    if (prec < MXB_PREC_FP64 || prec > MXB_PREC_SPLIT_BF16_X6) {
         set_error("unknown precision mode");
         return MXB_ERR_ARG;
     }
@@ -399,7 +399,7 @@ int Plan::create(const mxb_cds_desc &d, int prec, Plan **out)
         MXB_CUDA(cudaMemcpy(p->dItems, p->items.data(), p->items.size() * sizeof(Item), cudaMemcpyHostToDevice));
     rc = p->alloc((void **)&p->dOfs, 4 * (size_t)p->nleaf * sizeof(int32_t));
     if (rc) return rc;
-    if (prec == MXB_PREC_SPLIT_BF16) {
+    if (prec != MXB_PREC_FP64) {
         rc = p->setup_split_bf16(d);
         if (rc) return rc;
     }
@@ -476,7 +476,7 @@ int Plan::run(const std::vector<Launch> &L, const double *dW, double *dY, int nr
     if (rc) return rc;
     rc = stage_offsets(1, yofs, nrhs, stream);
     if (rc) return rc;
-    if (precision == MXB_PREC_SPLIT_BF16) return run_split_bf16(L, dW, dY, nrhs, accumulate, stream);
+    if (precision != MXB_PREC_FP64) return run_split_bf16(L, dW, dY, nrhs, accumulate, stream);
     Operands ops{};
     ops.pool[0] = dD;
     ops.pool[1] = dB;

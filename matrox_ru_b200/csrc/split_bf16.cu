@@ -17,10 +17,12 @@
 // projections and their transposes) are tiled once when the plan is created; W and the
 // skeleton vectors are tiled per evaluation by split kernels (HBM-bound passes).
 //
-// GEMM kernel: one CTA per (task row tile, 128|256 right-hand sides), 4 warps:
-//   warp 0 lane 0 : producer -- bulk copies of the A and B part tiles of each K step
-//   warp 1 lane 0 : MMA issuer -- tcgen05.mma M=128, N=BN, K=16, 3 or 6 per 16-K slice
-//   all 4 warps   : epilogue -- tcgen05.ld of the FP32 accumulator rows, coalesced stores
+// GEMM kernel: one CTA per (task row tile, 128|256 right-hand sides), 10 warps:
+//   warp 8 lane 0 : producer -- bulk copies of the A and B part tiles of each K step
+//   warp 9 lane 0 : MMA issuer -- tcgen05.mma M=128, N=BN, K=16, 3 or 6 per 16-K slice,
+//                   one fresh TMEM accumulator (of two) per 64-deep K tile
+//   warps 0-7     : drain every K tile's accumulator into round-to-nearest FP32 registers
+//                   (tcgen05.ld), then store rows with coalesced writes
 // Every wait is bounded (tc::WAIT_CYCLES); a CTA that times out raises MXB_ERR_TIMEOUT in
 // the plan's error word, drains its own copies and MMAs, frees its TMEM and exits.
 #include <algorithm>
@@ -35,7 +37,7 @@
 
 namespace mxb {
 
-int row_tile_for(int precision) { return precision == MXB_PREC_SPLIT_BF16 ? 128 : 64; }
+int row_tile_for(int precision) { return precision != MXB_PREC_FP64 ? 128 : 64; }
 
 namespace {
 
@@ -157,10 +159,19 @@ struct TcCfg {
     static constexpr int STAGE = A_BYTES + B_BYTES;
     static constexpr int SMEM = STAGES * STAGE + 1024 + 256;
     static constexpr int NPROD = P == 2 ? 3 : 6;
+    static constexpr int EPI_WARPS = 8;          // two per TMEM lane quarter, one per column half
+    static constexpr int THREADS = (EPI_WARPS + 2) * 32;
+    static constexpr int COLS = BN / 2;          // accumulator columns per epilogue thread
+    static constexpr int TMEM_COLS = 2 * BN;     // two accumulator buffers
 };
 
+// Tensor-core FP32 accumulation is not round-to-nearest: its error grows with the number of
+// MMAs chained into one accumulator (measured ~4e-5 relative after 8192-deep chains).  So
+// each 64-deep K tile gets a fresh TMEM accumulator (two buffers, alternating), and the
+// epilogue warps add every tile's partial sums into per-thread FP32 registers with ordinary
+// round-to-nearest adds while the tensor core already works on the next tile.
 template <int P, int BN>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(TcCfg<P, BN>::THREADS, 1)
 tc_gemm_kernel(const Task *__restrict__ tasks, const TcItem *__restrict__ items, TcArgs args)
 {
     using C = TcCfg<P, BN>;
@@ -168,8 +179,10 @@ tc_gemm_kernel(const Task *__restrict__ tasks, const TcItem *__restrict__ items,
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + C::STAGES * C::STAGE);
     uint64_t *empty = full + C::STAGES;
-    uint64_t *accb = empty + C::STAGES;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(accb + 1);
+    uint64_t *accf = empty + C::STAGES;  // accumulator buffer b holds a finished K tile
+    uint64_t *acce = accf + 2;           // accumulator buffer b has been drained
+    uint64_t *doneb = acce + 2;          // every MMA this CTA issued has completed
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(doneb + 1);
     volatile int *abort_word = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
     const Task t = tasks[blockIdx.x];
@@ -183,135 +196,169 @@ tc_gemm_kernel(const Task *__restrict__ tasks, const TcItem *__restrict__ items,
             tc::mbar_init(&full[s], 1);
             tc::mbar_init(&empty[s], 1);
         }
-        tc::mbar_init(accb, 1);
+        for (int b = 0; b < 2; ++b) {
+            tc::mbar_init(&accf[b], 1);
+            tc::mbar_init(&acce[b], C::EPI_WARPS);
+        }
+        tc::mbar_init(doneb, 1);
         *abort_word = 0;
         tc::fence_mbar_init();
     }
-    if (warp == 0) tc::tmem_alloc(tmem_slot, BN);
+    if (warp == 0) tc::tmem_alloc(tmem_slot, C::TMEM_COLS);
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = *tmem_slot;
 
-    if (warp == 0 && lane == 0 && ktiles > 0) {
-        // ---------------- producer ----------------
-        int q = 0, kt = 0, issued = 0;
-        const int mt = t.m0 / 128;
-        for (int i = 0; i < ktiles; ++i) {
-            const int s = i % C::STAGES;
-            const uint32_t round = (uint32_t)(i / C::STAGES);
-            if (!tc::mbar_wait(&empty[s], (round & 1) ^ 1, abort_word)) {
-                *abort_word = 1;
-                break;
-            }
-            while (kt >= ti[q].KT) {
-                ++q;
-                kt = 0;
-            }
-            const TcItem it = ti[q];
-            uint8_t *sa = smem + s * C::STAGE;
-            uint8_t *sb = sa + C::A_BYTES;
-            tc::mbar_expect_tx(&full[s], C::STAGE);
-            const uint8_t *ga = args.a_pool + it.a_off + ((size_t)mt * it.KT + kt) * (size_t)P * TILE_BYTES;
-            tc::bulk_g2s(sa, ga, C::A_BYTES, &full[s]);
+    float acc[C::COLS];
 #pragma unroll
-            for (int hh = 0; hh < C::HALVES; ++hh) {
-                const size_t nt = (size_t)blockIdx.y * C::HALVES + hh;
-                const uint8_t *gb = args.b_pool + ((size_t)it.b_base * args.NT + nt * it.KT + kt) * 3 * (size_t)TILE_BYTES;
+    for (int e = 0; e < C::COLS; ++e) acc[e] = 0.f;
+
+    if (warp == C::EPI_WARPS) {
+        if (lane == 0 && ktiles > 0) {
+            // ---------------- producer ----------------
+            int q = 0, kt = 0, issued = 0;
+            const int mt = t.m0 / 128;
+            for (int i = 0; i < ktiles; ++i) {
+                const int s = i % C::STAGES;
+                const uint32_t round = (uint32_t)(i / C::STAGES);
+                if (!tc::mbar_wait(&empty[s], (round & 1) ^ 1, abort_word)) {
+                    *abort_word = 1;
+                    break;
+                }
+                while (kt >= ti[q].KT) {
+                    ++q;
+                    kt = 0;
+                }
+                const TcItem it = ti[q];
+                uint8_t *sa = smem + s * C::STAGE;
+                uint8_t *sb = sa + C::A_BYTES;
+                tc::mbar_expect_tx(&full[s], C::STAGE);
+                const uint8_t *ga = args.a_pool + it.a_off + ((size_t)mt * it.KT + kt) * (size_t)P * TILE_BYTES;
+                tc::bulk_g2s(sa, ga, C::A_BYTES, &full[s]);
 #pragma unroll
-                for (int p = 0; p < P; ++p)
-                    tc::bulk_g2s(sb + (p * C::HALVES + hh) * TILE_BYTES, gb + (size_t)p * TILE_BYTES, TILE_BYTES, &full[s]);
+                for (int hh = 0; hh < C::HALVES; ++hh) {
+                    const size_t nt = (size_t)blockIdx.y * C::HALVES + hh;
+                    const uint8_t *gb =
+                        args.b_pool + ((size_t)it.b_base * args.NT + nt * it.KT + kt) * 3 * (size_t)TILE_BYTES;
+#pragma unroll
+                    for (int p = 0; p < P; ++p)
+                        tc::bulk_g2s(sb + (p * C::HALVES + hh) * TILE_BYTES, gb + (size_t)p * TILE_BYTES, TILE_BYTES,
+                                     &full[s]);
+                }
+                ++kt;
+                ++issued;
             }
-            ++kt;
-            ++issued;
+            // every stage this thread filled must have landed before the CTA may exit
+            for (int s = 0; s < C::STAGES && s < issued; ++s) {
+                const uint32_t last_round = (uint32_t)((issued - 1 - s) / C::STAGES);
+                volatile int never = 0;
+                tc::mbar_wait(&full[s], last_round & 1, &never);
+            }
         }
-        // drain: every stage this thread filled must have landed before the CTA may exit
-        for (int s = 0; s < C::STAGES && s < issued; ++s) {
-            const uint32_t last_round = (uint32_t)((issued - 1 - s) / C::STAGES);
-            volatile int never = 0;
-            tc::mbar_wait(&full[s], last_round & 1, &never);
+    } else if (warp == C::EPI_WARPS + 1) {
+        if (lane == 0 && ktiles > 0) {
+            // ---------------- MMA issuer ----------------
+            constexpr uint32_t IDESC = tc::idesc_bf16_f32(128, BN);
+            constexpr int PA[6] = {0, 0, 1, 0, 1, 2};
+            constexpr int PB[6] = {0, 1, 0, 2, 1, 0};
+            for (int i = 0; i < ktiles; ++i) {
+                const int s = i % C::STAGES;
+                const uint32_t round = (uint32_t)(i / C::STAGES);
+                const int b = i & 1;
+                const uint32_t use = (uint32_t)(i >> 1);
+                if (!tc::mbar_wait(&acce[b], (use & 1) ^ 1, abort_word) ||
+                    !tc::mbar_wait(&full[s], round & 1, abort_word)) {
+                    *abort_word = 1;
+                    break;
+                }
+                tc::fence_after_sync();
+                const uint32_t sa = tc::smem_u32(smem + s * C::STAGE);
+                const uint32_t sb = sa + C::A_BYTES;
+                const uint32_t dst = tmem + (uint32_t)(b * BN);
+                uint32_t accum = 0;
+#pragma unroll
+                for (int ks = 0; ks < 4; ++ks) {
+#pragma unroll
+                    for (int j = 0; j < C::NPROD; ++j) {
+                        const uint64_t ad = tc::smem_desc_sw128(sa + PA[j] * TILE_BYTES + ks * 32);
+                        const uint64_t bd = tc::smem_desc_sw128(sb + PB[j] * C::HALVES * TILE_BYTES + ks * 32);
+                        tc::mma_bf16(dst, ad, bd, IDESC, accum);
+                        accum = 1;
+                    }
+                }
+                tc::mma_commit(&empty[s]);
+                tc::mma_commit(&accf[b]);
+            }
+            tc::mma_commit(doneb);
         }
-    } else if (warp == 1 && lane == 0 && ktiles > 0) {
-        // ---------------- MMA issuer ----------------
-        constexpr uint32_t IDESC = tc::idesc_bf16_f32(128, BN);
-        constexpr int PA[6] = {0, 0, 1, 0, 1, 2};
-        constexpr int PB[6] = {0, 1, 0, 2, 1, 0};
-        uint32_t acc = 0;
+    } else {
+        // ---------------- epilogue warps: drain each K tile into registers ----------------
+        const int quarter = warp & 3, half = warp >> 2;
+        const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
         for (int i = 0; i < ktiles; ++i) {
-            const int s = i % C::STAGES;
-            const uint32_t round = (uint32_t)(i / C::STAGES);
-            if (!tc::mbar_wait(&full[s], round & 1, abort_word)) {
+            const int b = i & 1;
+            const uint32_t use = (uint32_t)(i >> 1);
+            if (!tc::mbar_wait(&accf[b], use & 1, abort_word)) {
                 *abort_word = 1;
                 break;
             }
             tc::fence_after_sync();
-            const uint32_t sa = tc::smem_u32(smem + s * C::STAGE);
-            const uint32_t sb = sa + C::A_BYTES;
 #pragma unroll
-            for (int ks = 0; ks < 4; ++ks) {
+            for (int c0 = 0; c0 < C::COLS; c0 += 32) {
+                float v[32];
+                tc::tmem_ld32(tmem + lane_base + (uint32_t)(b * BN + half * C::COLS + c0), v);
 #pragma unroll
-                for (int j = 0; j < C::NPROD; ++j) {
-                    const uint64_t ad = tc::smem_desc_sw128(sa + PA[j] * TILE_BYTES + ks * 32);
-                    const uint64_t bd = tc::smem_desc_sw128(sb + PB[j] * C::HALVES * TILE_BYTES + ks * 32);
-                    tc::mma_bf16(tmem, ad, bd, IDESC, acc);
-                    acc = 1;
-                }
+                for (int e = 0; e < 32; ++e) acc[c0 + e] += v[e];
             }
-            tc::mma_commit(&empty[s]);
+            tc::fence_before_sync();
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(tc::smem_u32(&acce[b])) : "memory");
         }
-        tc::mma_commit(accb);  // arrives once every MMA issued above has completed
     }
     __syncwarp();
-
-    // ---------------- epilogue ----------------
-    if (ktiles > 0) {
-        volatile int never = 0;  // a timed-out CTA still waits (bounded) for its MMAs
-        if (!tc::mbar_wait(accb, 0, &never)) *abort_word = 1;
+    __syncthreads();
+    // all MMAs must be complete before TMEM is released (bounded, also after an abort)
+    if (ktiles > 0 && threadIdx.x == 0) {
+        volatile int never = 0;
+        if (!tc::mbar_wait(doneb, 0, &never)) *abort_word = 1;
     }
-    __syncthreads();  // makes `aborted` (and so the tcgen05.ld below) uniform across the CTA
-    tc::fence_after_sync();
+    __syncthreads();
     const bool aborted = *abort_word != 0;
-    const bool have = ktiles > 0 && !aborted;
     if (aborted && threadIdx.x == 0) atomicExch(args.err, MXB_ERR_TIMEOUT);
-    const int r = t.m0 + warp * 32 + lane;
-    const bool row_ok = r < t.M && !aborted;
-    const int beta = t.beta == 2 ? args.beta_arg : t.beta;
-    const int col0 = blockIdx.y * BN;
-#pragma unroll 1
-    for (int c0 = 0; c0 < BN; c0 += 32) {
-        float v[32];
-        if (have) {
-            tc::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-        } else {
+
+    if (warp < C::EPI_WARPS && !aborted) {
+        const int quarter = warp & 3, half = warp >> 2;
+        const int r = t.m0 + quarter * 32 + lane;
+        if (r < t.M) {
+            const int beta = t.beta == 2 ? args.beta_arg : t.beta;
+            const int col0 = blockIdx.y * BN + half * C::COLS;
+            if (args.out_kind == 0) {
+                double *Yb = args.Y + args.yofs[t.c_row] + r;
 #pragma unroll
-            for (int e = 0; e < 32; ++e) v[e] = 0.f;
-        }
-        if (!row_ok) continue;
-        if (args.out_kind == 0) {
-            double *Yb = args.Y + args.yofs[t.c_row] + r;
-#pragma unroll
-            for (int e = 0; e < 32; ++e) {
-                const int col = col0 + c0 + e;
-                if (col < args.nrhs) {
-                    double *p = Yb + (size_t)col * t.ldc;
-                    *p = beta ? *p + (double)v[e] : (double)v[e];
+                for (int e = 0; e < C::COLS; ++e) {
+                    const int col = col0 + e;
+                    if (col < args.nrhs) {
+                        double *p = Yb + (size_t)col * t.ldc;
+                        *p = beta ? *p + (double)acc[e] : (double)acc[e];
+                    }
                 }
-            }
-        } else {
-            float *Sb = args.skel + t.c_row * (int64_t)args.nrhs + r;
+            } else {
+                float *Sb = args.skel + t.c_row * (int64_t)args.nrhs + r;
 #pragma unroll
-            for (int e = 0; e < 32; ++e) {
-                const int col = col0 + c0 + e;
-                if (col < args.nrhs) {
-                    float *p = Sb + (size_t)col * t.ldc;
-                    *p = beta ? *p + v[e] : v[e];
+                for (int e = 0; e < C::COLS; ++e) {
+                    const int col = col0 + e;
+                    if (col < args.nrhs) {
+                        float *p = Sb + (size_t)col * t.ldc;
+                        *p = beta ? *p + acc[e] : acc[e];
+                    }
                 }
             }
         }
     }
     tc::fence_before_sync();
     __syncthreads();
-    if (warp == 0) tc::tmem_dealloc(tmem, BN);
+    if (warp == 0) tc::tmem_dealloc(tmem, C::TMEM_COLS);
 }
 
 template <int P, int BN>
@@ -322,12 +369,12 @@ cudaError_t launch_tc(const Task *tasks, const TcItem *items, int ntasks, const 
     cudaError_t e = cudaFuncSetAttribute(tc_gemm_kernel<P, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
     if (e != cudaSuccess) return e;
     dim3 grid(ntasks, (a.nrhs + BN - 1) / BN);
-    tc_gemm_kernel<P, BN><<<grid, 128, C::SMEM, s>>>(tasks, items, a);
+    tc_gemm_kernel<P, BN><<<grid, C::THREADS, C::SMEM, s>>>(tasks, items, a);
     return cudaGetLastError();
 }
 
 enum OpKind { OP_SPLIT_W, OP_SPLIT_WSKEL, OP_SPLIT_USKEL, OP_TC2, OP_TC3 };
-enum APool { POOL_D2, POOL_F2, POOL_VU3, POOL_VD3, NPOOL };
+enum APool { POOL_NEAR, POOL_FAR, POOL_VU3, POOL_VD3, NPOOL };
 enum BBuf { BUF_W, BUF_WSKEL, BUF_USKEL };
 
 struct Op {
@@ -361,6 +408,9 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
 {
     SplitBF16 *S = new SplitBF16();
     bf16 = S;
+    // bf16x3 (2 stored parts) or bf16x6 (3 parts) for the near field and the far couplings
+    const int near_parts = precision == MXB_PREC_SPLIT_BF16_X6 ? 3 : 2;
+    const int far_parts = precision == MXB_PREC_SPLIT_BF16 ? 2 : 3;
     auto KT = [](int64_t k) { return (int32_t)ceil_div(std::max<int64_t>(k, 0), 64); };
     auto RT = [](int64_t r) { return (int32_t)ceil_div(std::max<int64_t>(r, 0), 128); };
     auto projects = [&](int v) { return v != root && slen[v] > 0; };
@@ -397,9 +447,9 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
     };
     std::vector<uint64_t> near_a(near_x.size()), far_a(far_x.size());
     for (size_t k = 0; k < near_x.size(); ++k)
-        near_a[k] = add_pool(POOL_D2, 0, near_off[k], Ddim[near_x[k]], Ddim[near_x[k]], Ddim[near_y[k]], 0, 2);
+        near_a[k] = add_pool(POOL_NEAR, 0, near_off[k], Ddim[near_x[k]], Ddim[near_x[k]], Ddim[near_y[k]], 0, near_parts);
     for (size_t k = 0; k < far_x.size(); ++k)
-        far_a[k] = add_pool(POOL_F2, 1, far_off[k], slen[far_x[k]], slen[far_x[k]], slen[far_y[k]], 0, 2);
+        far_a[k] = add_pool(POOL_FAR, 1, far_off[k], slen[far_x[k]], slen[far_x[k]], slen[far_y[k]], 0, far_parts);
     std::vector<uint64_t> up_a(numnodes), up_b(numnodes), down_a(numnodes);
     for (int v = 0; v < numnodes; ++v) {
         if (!projects(v)) continue;
@@ -527,7 +577,7 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
     std::vector<std::vector<int>> far_out(numnodes);
     for (size_t k = 0; k < far_x.size(); ++k) far_out[far_x[k]].push_back((int)k);
     for (int dd = 1; dd <= maxd; ++dd) {
-        begin_op(OP_TC2, POOL_F2, BUF_WSKEL, 1);
+        begin_op(far_parts == 2 ? OP_TC2 : OP_TC3, POOL_FAR, BUF_WSKEL, 1);
         for (int c : bfs) {
             if (depth[c] != dd || !projects(c)) continue;
             const int item0 = (int)S->items.size();
@@ -556,7 +606,7 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
     // near (Y (+)= D W) then leaf down (Y += P^T uskel)
     std::vector<std::vector<int>> near_out(nleaf);
     for (size_t k = 0; k < near_x.size(); ++k) near_out[near_x[k]].push_back((int)k);
-    begin_op(OP_TC2, POOL_D2, BUF_W, 0);
+    begin_op(near_parts == 2 ? OP_TC2 : OP_TC3, POOL_NEAR, BUF_W, 0);
     for (int v : bfs) {
         if (lch[v] != -1) continue;
         const int x = lm[v];

@@ -17,7 +17,8 @@ import numpy as np
 from . import _lib
 from ._lib import P, I32, check
 
-PRECISIONS = {"fp64": _lib.PREC_FP64, "split_bf16": _lib.PREC_SPLIT_BF16}
+PRECISIONS = {"fp64": _lib.PREC_FP64, "split_bf16": _lib.PREC_SPLIT_BF16,
+              "split_bf16_far6": _lib.PREC_SPLIT_BF16_FAR6, "split_bf16_x6": _lib.PREC_SPLIT_BF16_X6}
 
 
 def _np(a, dt):

@@ -27,10 +27,10 @@ def frob(a, b):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
-def run_plan(torch, cds, r, seed=0):
+def run_plan(torch, cds, r, seed=0, mode="split_bf16"):
     TW = np.random.default_rng(seed).standard_normal(cds.n * r)
     want = O.eval_h2b(cds, TW, r)
-    plan = H.Plan(cds, "split_bf16")
+    plan = H.Plan(cds, mode)
     got = plan.evaluate(torch.as_tensor(TW, device="cuda"), r)
     plan.status()
     return got.cpu().numpy(), want, plan
@@ -49,6 +49,15 @@ def test_split_matches_fp64(torch, small_cases, name, nrhs):
     got, want, _ = run_plan(torch, small_cases[name], nrhs, seed=nrhs)
     err = frob(got, want)
     assert 1e-12 < err <= TOL, err
+
+
+@pytest.mark.parametrize("mode", ["split_bf16_far6", "split_bf16_x6"])
+@pytest.mark.parametrize("name", ["hss", "h2b", "ragged"])
+def test_split_modes_with_six_products(torch, small_cases, name, mode):
+    """6-product far couplings (and near, for x6): x6 reaches FP32-level error."""
+    got, want, _ = run_plan(torch, small_cases[name], 70, seed=1, mode=mode)
+    err = frob(got, want)
+    assert 1e-12 < err <= (TOL if mode == "split_bf16_far6" else 5e-6), err
 
 
 def test_split_accumulate_and_repeat(torch, small_cases):
