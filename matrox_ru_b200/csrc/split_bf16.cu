@@ -170,9 +170,14 @@ struct TcCfg {
 // each 64-deep K tile gets a fresh TMEM accumulator (two buffers, alternating), and the
 // epilogue warps add every tile's partial sums into per-thread FP32 registers with ordinary
 // round-to-nearest adds while the tensor core already works on the next tile.
+//
+// Persistent: one CTA per SM walks the work units u = blockIdx.x, blockIdx.x + gridDim.x, ...
+// (unit = task x column tile).  The three roles walk the same sequence, so one global K-tile
+// counter drives every stage and accumulator phase; TMEM and the barriers are set up once,
+// and the epilogue of one unit overlaps the MMAs of the next.
 template <int P, int BN>
 __global__ void __launch_bounds__(TcCfg<P, BN>::THREADS, 1)
-tc_gemm_kernel(const Task *__restrict__ tasks, const TcItem *__restrict__ items, TcArgs args)
+tc_gemm_kernel(const Task *__restrict__ tasks, const TcItem *__restrict__ items, int nunits, TcArgs args)
 {
     using C = TcCfg<P, BN>;
     extern __shared__ uint8_t smem_raw[];
@@ -185,11 +190,8 @@ tc_gemm_kernel(const Task *__restrict__ tasks, const TcItem *__restrict__ items,
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(doneb + 1);
     volatile int *abort_word = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
-    const Task t = tasks[blockIdx.x];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const TcItem *ti = items + t.item0;
-    int ktiles = 0;
-    for (int q = 0; q < t.nitem; ++q) ktiles += ti[q].KT;
+    const int ncol = (args.nrhs + BN - 1) / BN;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < C::STAGES; ++s) {
@@ -210,166 +212,207 @@ tc_gemm_kernel(const Task *__restrict__ tasks, const TcItem *__restrict__ items,
     tc::fence_after_sync();
     const uint32_t tmem = *tmem_slot;
 
-    float acc[C::COLS];
-#pragma unroll
-    for (int e = 0; e < C::COLS; ++e) acc[e] = 0.f;
-
     if (warp == C::EPI_WARPS) {
-        if (lane == 0 && ktiles > 0) {
+        if (lane == 0) {
             // ---------------- producer ----------------
-            int q = 0, kt = 0, issued = 0;
-            const int mt = t.m0 / 128;
-            for (int i = 0; i < ktiles; ++i) {
-                const int s = i % C::STAGES;
-                const uint32_t round = (uint32_t)(i / C::STAGES);
-                if (!tc::mbar_wait(&empty[s], (round & 1) ^ 1, abort_word)) {
-                    *abort_word = 1;
-                    break;
-                }
-                while (kt >= ti[q].KT) {
-                    ++q;
-                    kt = 0;
-                }
-                const TcItem it = ti[q];
-                uint8_t *sa = smem + s * C::STAGE;
-                uint8_t *sb = sa + C::A_BYTES;
-                tc::mbar_expect_tx(&full[s], C::STAGE);
-                const uint8_t *ga = args.a_pool + it.a_off + ((size_t)mt * it.KT + kt) * (size_t)P * TILE_BYTES;
-                tc::bulk_g2s(sa, ga, C::A_BYTES, &full[s]);
+            uint32_t g = 0;  // global K-tile counter of this CTA
+            for (int u = blockIdx.x; u < nunits && !*abort_word; u += gridDim.x) {
+                const Task t = tasks[u / ncol];
+                const int col = u % ncol;
+                const TcItem *ti = items + t.item0;
+                const int mt = t.m0 / 128;
+                for (int q = 0; q < t.nitem && !*abort_word; ++q) {
+                    const TcItem it = ti[q];
+                    for (int kt = 0; kt < it.KT; ++kt, ++g) {
+                        const int s = g % C::STAGES;
+                        const uint32_t round = g / C::STAGES;
+                        if (!tc::mbar_wait(&empty[s], (round & 1) ^ 1, abort_word)) {
+                            *abort_word = 1;
+                            break;
+                        }
+                        uint8_t *sa = smem + s * C::STAGE;
+                        uint8_t *sb = sa + C::A_BYTES;
+                        tc::mbar_expect_tx(&full[s], C::STAGE);
+                        const uint8_t *ga =
+                            args.a_pool + it.a_off + ((size_t)mt * it.KT + kt) * (size_t)P * TILE_BYTES;
+                        tc::bulk_g2s(sa, ga, C::A_BYTES, &full[s]);
 #pragma unroll
-                for (int hh = 0; hh < C::HALVES; ++hh) {
-                    const size_t nt = (size_t)blockIdx.y * C::HALVES + hh;
-                    const uint8_t *gb =
-                        args.b_pool + ((size_t)it.b_base * args.NT + nt * it.KT + kt) * 3 * (size_t)TILE_BYTES;
+                        for (int hh = 0; hh < C::HALVES; ++hh) {
+                            const size_t nt = (size_t)col * C::HALVES + hh;
+                            const uint8_t *gb = args.b_pool +
+                                                ((size_t)it.b_base * args.NT + nt * it.KT + kt) * 3 * (size_t)TILE_BYTES;
 #pragma unroll
-                    for (int p = 0; p < P; ++p)
-                        tc::bulk_g2s(sb + (p * C::HALVES + hh) * TILE_BYTES, gb + (size_t)p * TILE_BYTES, TILE_BYTES,
-                                     &full[s]);
+                            for (int p = 0; p < P; ++p)
+                                tc::bulk_g2s(sb + (p * C::HALVES + hh) * TILE_BYTES, gb + (size_t)p * TILE_BYTES,
+                                             TILE_BYTES, &full[s]);
+                        }
+                    }
                 }
-                ++kt;
-                ++issued;
             }
             // every stage this thread filled must have landed before the CTA may exit
-            for (int s = 0; s < C::STAGES && s < issued; ++s) {
-                const uint32_t last_round = (uint32_t)((issued - 1 - s) / C::STAGES);
+            for (int s = 0; s < C::STAGES && (uint32_t)s < g; ++s) {
+                const uint32_t last_round = (g - 1 - s) / C::STAGES;
                 volatile int never = 0;
                 tc::mbar_wait(&full[s], last_round & 1, &never);
             }
         }
     } else if (warp == C::EPI_WARPS + 1) {
-        if (lane == 0 && ktiles > 0) {
+        if (lane == 0) {
             // ---------------- MMA issuer ----------------
             constexpr uint32_t IDESC = tc::idesc_bf16_f32(128, BN);
             constexpr int PA[6] = {0, 0, 1, 0, 1, 2};
             constexpr int PB[6] = {0, 1, 0, 2, 1, 0};
-            for (int i = 0; i < ktiles; ++i) {
-                const int s = i % C::STAGES;
-                const uint32_t round = (uint32_t)(i / C::STAGES);
-                const int b = i & 1;
-                const uint32_t use = (uint32_t)(i >> 1);
-                if (!tc::mbar_wait(&acce[b], (use & 1) ^ 1, abort_word) ||
-                    !tc::mbar_wait(&full[s], round & 1, abort_word)) {
+            uint32_t g = 0;
+            bool any = false;
+            for (int u = blockIdx.x; u < nunits && !*abort_word; u += gridDim.x) {
+                const Task t = tasks[u / ncol];
+                int ktiles = 0;
+                for (int q = 0; q < t.nitem; ++q) ktiles += items[t.item0 + q].KT;
+                for (int i = 0; i < ktiles; ++i, ++g) {
+                    const int s = g % C::STAGES;
+                    const uint32_t round = g / C::STAGES;
+                    const int b = g & 1;
+                    const uint32_t use = g >> 1;
+                    if (!tc::mbar_wait(&acce[b], (use & 1) ^ 1, abort_word) ||
+                        !tc::mbar_wait(&full[s], round & 1, abort_word)) {
+                        *abort_word = 1;
+                        break;
+                    }
+                    tc::fence_after_sync();
+                    const uint32_t sa = tc::smem_u32(smem + s * C::STAGE);
+                    const uint32_t sb = sa + C::A_BYTES;
+                    const uint32_t dst = tmem + (uint32_t)(b * BN);
+                    uint32_t accum = 0;
+#pragma unroll
+                    for (int ks = 0; ks < 4; ++ks) {
+#pragma unroll
+                        for (int j = 0; j < C::NPROD; ++j) {
+                            const uint64_t ad = tc::smem_desc_sw128(sa + PA[j] * TILE_BYTES + ks * 32);
+                            const uint64_t bd = tc::smem_desc_sw128(sb + PB[j] * C::HALVES * TILE_BYTES + ks * 32);
+                            tc::mma_bf16(dst, ad, bd, IDESC, accum);
+                            accum = 1;
+                        }
+                    }
+                    tc::mma_commit(&empty[s]);
+                    tc::mma_commit(&accf[b]);
+                    any = true;
+                }
+            }
+            if (any) tc::mma_commit(doneb);
+            else tc::mbar_expect_tx(doneb, 0);  // nothing issued: complete the barrier's phase now
+        }
+    } else {
+        // ---------------- epilogue warps ----------------
+        const int quarter = warp & 3, half = warp >> 2;
+        const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
+        uint32_t g = 0;
+        for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+            const Task t = tasks[u / ncol];
+            const int col = u % ncol;
+            int ktiles = 0;
+            for (int q = 0; q < t.nitem; ++q) ktiles += items[t.item0 + q].KT;
+            float acc[C::COLS];
+#pragma unroll
+            for (int e = 0; e < C::COLS; ++e) acc[e] = 0.f;
+            bool ok = !*abort_word;
+            for (int i = 0; i < ktiles && ok; ++i, ++g) {
+                const int b = g & 1;
+                const uint32_t use = g >> 1;
+                if (!tc::mbar_wait(&accf[b], use & 1, abort_word)) {
                     *abort_word = 1;
+                    ok = false;
                     break;
                 }
                 tc::fence_after_sync();
-                const uint32_t sa = tc::smem_u32(smem + s * C::STAGE);
-                const uint32_t sb = sa + C::A_BYTES;
-                const uint32_t dst = tmem + (uint32_t)(b * BN);
-                uint32_t accum = 0;
 #pragma unroll
-                for (int ks = 0; ks < 4; ++ks) {
+                for (int c0 = 0; c0 < C::COLS; c0 += 32) {
+                    float v[32];
+                    tc::tmem_ld32(tmem + lane_base + (uint32_t)(b * BN + half * C::COLS + c0), v);
 #pragma unroll
-                    for (int j = 0; j < C::NPROD; ++j) {
-                        const uint64_t ad = tc::smem_desc_sw128(sa + PA[j] * TILE_BYTES + ks * 32);
-                        const uint64_t bd = tc::smem_desc_sw128(sb + PB[j] * C::HALVES * TILE_BYTES + ks * 32);
-                        tc::mma_bf16(dst, ad, bd, IDESC, accum);
-                        accum = 1;
+                    for (int e = 0; e < 32; ++e) acc[c0 + e] += v[e];
+                }
+                tc::fence_before_sync();
+                __syncwarp();
+                if (lane == 0)
+                    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(tc::smem_u32(&acce[b])) : "memory");
+            }
+            if (!ok || *abort_word) break;
+            const int r = t.m0 + quarter * 32 + lane;
+            if (r < t.M) {
+                const int beta = t.beta == 2 ? args.beta_arg : t.beta;
+                const int col0 = col * BN + half * C::COLS;
+                // accumulating outputs: all old values of a 16-column chunk are loaded before
+                // any store, so the loads overlap instead of waiting on each other
+                if (args.out_kind == 0) {
+                    double *Yb = args.Y + args.yofs[t.c_row] + r;
+#pragma unroll
+                    for (int c0 = 0; c0 < C::COLS; c0 += 16) {
+                        double old[16];
+#pragma unroll
+                        for (int e = 0; e < 16; ++e) {
+                            const int cc = col0 + c0 + e;
+                            old[e] = (beta && cc < args.nrhs) ? Yb[(size_t)cc * t.ldc] : 0.0;
+                        }
+#pragma unroll
+                        for (int e = 0; e < 16; ++e) {
+                            const int cc = col0 + c0 + e;
+                            if (cc < args.nrhs) Yb[(size_t)cc * t.ldc] = old[e] + (double)acc[c0 + e];
+                        }
+                    }
+                } else {
+                    float *Sb = args.skel + t.c_row * (int64_t)args.nrhs + r;
+#pragma unroll
+                    for (int c0 = 0; c0 < C::COLS; c0 += 16) {
+                        float old[16];
+#pragma unroll
+                        for (int e = 0; e < 16; ++e) {
+                            const int cc = col0 + c0 + e;
+                            old[e] = (beta && cc < args.nrhs) ? Sb[(size_t)cc * t.ldc] : 0.f;
+                        }
+#pragma unroll
+                        for (int e = 0; e < 16; ++e) {
+                            const int cc = col0 + c0 + e;
+                            if (cc < args.nrhs) Sb[(size_t)cc * t.ldc] = old[e] + acc[c0 + e];
+                        }
                     }
                 }
-                tc::mma_commit(&empty[s]);
-                tc::mma_commit(&accf[b]);
             }
-            tc::mma_commit(doneb);
-        }
-    } else {
-        // ---------------- epilogue warps: drain each K tile into registers ----------------
-        const int quarter = warp & 3, half = warp >> 2;
-        const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
-        for (int i = 0; i < ktiles; ++i) {
-            const int b = i & 1;
-            const uint32_t use = (uint32_t)(i >> 1);
-            if (!tc::mbar_wait(&accf[b], use & 1, abort_word)) {
-                *abort_word = 1;
-                break;
-            }
-            tc::fence_after_sync();
-#pragma unroll
-            for (int c0 = 0; c0 < C::COLS; c0 += 32) {
-                float v[32];
-                tc::tmem_ld32(tmem + lane_base + (uint32_t)(b * BN + half * C::COLS + c0), v);
-#pragma unroll
-                for (int e = 0; e < 32; ++e) acc[c0 + e] += v[e];
-            }
-            tc::fence_before_sync();
-            __syncwarp();
-            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(tc::smem_u32(&acce[b])) : "memory");
         }
     }
     __syncwarp();
     __syncthreads();
     // all MMAs must be complete before TMEM is released (bounded, also after an abort)
-    if (ktiles > 0 && threadIdx.x == 0) {
+    if (threadIdx.x == 0) {
         volatile int never = 0;
         if (!tc::mbar_wait(doneb, 0, &never)) *abort_word = 1;
     }
     __syncthreads();
-    const bool aborted = *abort_word != 0;
-    if (aborted && threadIdx.x == 0) atomicExch(args.err, MXB_ERR_TIMEOUT);
-
-    if (warp < C::EPI_WARPS && !aborted) {
-        const int quarter = warp & 3, half = warp >> 2;
-        const int r = t.m0 + quarter * 32 + lane;
-        if (r < t.M) {
-            const int beta = t.beta == 2 ? args.beta_arg : t.beta;
-            const int col0 = blockIdx.y * BN + half * C::COLS;
-            if (args.out_kind == 0) {
-                double *Yb = args.Y + args.yofs[t.c_row] + r;
-#pragma unroll
-                for (int e = 0; e < C::COLS; ++e) {
-                    const int col = col0 + e;
-                    if (col < args.nrhs) {
-                        double *p = Yb + (size_t)col * t.ldc;
-                        *p = beta ? *p + (double)acc[e] : (double)acc[e];
-                    }
-                }
-            } else {
-                float *Sb = args.skel + t.c_row * (int64_t)args.nrhs + r;
-#pragma unroll
-                for (int e = 0; e < C::COLS; ++e) {
-                    const int col = col0 + e;
-                    if (col < args.nrhs) {
-                        float *p = Sb + (size_t)col * t.ldc;
-                        *p = beta ? *p + acc[e] : acc[e];
-                    }
-                }
-            }
-        }
-    }
+    if (*abort_word && threadIdx.x == 0) atomicExch(args.err, MXB_ERR_TIMEOUT);
     tc::fence_before_sync();
     __syncthreads();
     if (warp == 0) tc::tmem_dealloc(tmem, C::TMEM_COLS);
 }
+
+int g_sm_count[128];
 
 template <int P, int BN>
 cudaError_t launch_tc(const Task *tasks, const TcItem *items, int ntasks, const TcArgs &a, cudaStream_t s)
 {
     if (ntasks <= 0) return cudaSuccess;
     using C = TcCfg<P, BN>;
-    cudaError_t e = cudaFuncSetAttribute(tc_gemm_kernel<P, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    dim3 grid(ntasks, (a.nrhs + BN - 1) / BN);
-    tc_gemm_kernel<P, BN><<<grid, C::THREADS, C::SMEM, s>>>(tasks, items, a);
+    if (dev < 0 || dev >= 128) return cudaErrorInvalidDevice;
+    if (!g_sm_count[dev]) {
+        e = cudaDeviceGetAttribute(&g_sm_count[dev], cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return e;
+    }
+    e = cudaFuncSetAttribute(tc_gemm_kernel<P, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
+    if (e != cudaSuccess) return e;
+    const int nunits = ntasks * ((a.nrhs + BN - 1) / BN);
+    const int grid = std::min(nunits, g_sm_count[dev]);
+    tc_gemm_kernel<P, BN><<<grid, C::THREADS, C::SMEM, s>>>(tasks, items, nunits, a);
     return cudaGetLastError();
 }
 
@@ -512,6 +555,16 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
     };
     auto end_op = [&]() {
         Op &o = S->ops.back();
+        if (o.kind >= OP_TC2) {
+            // longest tasks first: balances the persistent kernel's static round-robin
+            auto cost = [&](const Task &t) {
+                int k = 0;
+                for (int q = 0; q < t.nitem; ++q) k += S->items[t.item0 + q].KT;
+                return k;
+            };
+            std::stable_sort(S->tasks.begin() + o.first, S->tasks.end(),
+                             [&](const Task &a, const Task &b) { return cost(a) > cost(b); });
+        }
         o.count = ((o.kind <= OP_SPLIT_USKEL) ? (int)S->jobs.size() : (int)S->tasks.size()) - o.first;
         o.max_kt = 1;
         if (o.kind <= OP_SPLIT_USKEL)
