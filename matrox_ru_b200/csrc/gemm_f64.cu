@@ -197,19 +197,29 @@ gemm_f64_kernel(const Task *__restrict__ tasks, const Item *__restrict__ items, 
 cudaError_t launch_gemm_f64(const Task *tasks, const Item *items, int ntasks, const Operands &ops,
                             cudaStream_t stream)
 {
-    if (ntasks <= 0) return cudaSuccess;
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(gemm_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)SMEM_BYTES);
+    static bool configured[128];
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 128) return cudaErrorInvalidDevice;
+    if (!configured[dev]) {
+        e = cudaFuncSetAttribute(gemm_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES);
         if (e != cudaSuccess) return e;
-        configured = true;
+        configured[dev] = true;
     }
+    if (ntasks <= 0) return cudaSuccess;
     dim3 grid(ntasks, (ops.nrhs + BN - 1) / BN);
     gemm_f64_kernel<<<grid, THREADS, SMEM_BYTES, stream>>>(tasks, items, ops);
     return cudaGetLastError();
 }
 
 int f64_row_tile() { return BM; }
+
+cudaError_t prepare_gemm_f64()
+{
+    Operands ops{};
+    ops.nrhs = 1;
+    return launch_gemm_f64(nullptr, nullptr, 0, ops, 0) == cudaSuccess ? cudaSuccess : cudaErrorUnknown;
+}
 
 }  // namespace mxb

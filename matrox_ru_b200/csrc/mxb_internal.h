@@ -70,6 +70,8 @@ struct Plan;
 cudaError_t launch_gemm_f64(const Task *tasks, const Item *items, int ntasks,
                             const Operands &ops, cudaStream_t stream);
 
+cudaError_t prepare_gemm_f64();  // sets the kernel's shared-memory limit (before any capture)
+
 void set_error(const std::string &msg);
 
 }  // namespace mxb

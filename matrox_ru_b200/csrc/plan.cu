@@ -12,6 +12,7 @@
 // exactly once per evaluation.  The adjoint reuses phases 1-2 on G and runs phases 3-4
 // with every near block and far coupling transposed.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -45,6 +46,8 @@ int row_tile_for(int precision);
 
 Plan::~Plan()
 {
+    clear_graphs();
+    if (capture_stream) cudaStreamDestroy(capture_stream);
     free_split_bf16();
     for (void *p : allocations) cudaFree(p);
 }
@@ -407,10 +410,17 @@ int Plan::create(const mxb_cds_desc &d, int prec, Plan **out)
     return MXB_OK;
 }
 
+void Plan::clear_graphs()
+{
+    for (GraphEntry &g : graphs) cudaGraphExecDestroy(g.exec);
+    graphs.clear();
+}
+
 int Plan::ensure_scratch(int nrhs)
 {
     const size_t need = (size_t)std::max<int64_t>(skel_total, 1) * nrhs;
     if (need <= scratch_elems) return MXB_OK;
+    clear_graphs();
     if (dWskel) {
         cudaFree(dWskel);
         cudaFree(dUskel);
@@ -476,6 +486,58 @@ int Plan::run(const std::vector<Launch> &L, const double *dW, double *dY, int nr
     if (rc) return rc;
     rc = stage_offsets(1, yofs, nrhs, stream);
     if (rc) return rc;
+    if (precision != MXB_PREC_FP64) {
+        bool realloc = false;
+        rc = prepare_split_bf16(nrhs, &realloc);
+        if (rc) return rc;
+        if (realloc) clear_graphs();
+    } else {
+        MXB_CUDA(prepare_gemm_f64());
+    }
+    static const bool use_graphs = [] {
+        const char *e = getenv("MXB_NO_GRAPHS");
+        return !(e && *e && *e != '0');
+    }();
+    if (!use_graphs) return enqueue(L, dW, dY, nrhs, accumulate, stream);
+    // replay a captured graph of the whole evaluation: one launch instead of dozens
+    GraphEntry *hit = nullptr;
+    for (GraphEntry &g : graphs)
+        if (g.launches == &L && g.W == dW && g.Y == dY && g.nrhs == nrhs && g.accumulate == accumulate) hit = &g;
+    if (!hit) {
+        if (!capture_stream) MXB_CUDA(cudaStreamCreateWithFlags(&capture_stream, cudaStreamNonBlocking));
+        MXB_CUDA(cudaStreamBeginCapture(capture_stream, cudaStreamCaptureModeThreadLocal));
+        rc = enqueue(L, dW, dY, nrhs, accumulate, capture_stream);
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(capture_stream, &graph);
+        if (rc) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        if (e != cudaSuccess) {
+            set_error(std::string("capturing the evaluation graph: ") + cudaGetErrorString(e));
+            return MXB_ERR_CUDA;
+        }
+        cudaGraphExec_t exec = nullptr;
+        e = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            set_error(std::string("instantiating the evaluation graph: ") + cudaGetErrorString(e));
+            return MXB_ERR_CUDA;
+        }
+        if (graphs.size() >= 8) {
+            cudaGraphExecDestroy(graphs.front().exec);
+            graphs.erase(graphs.begin());
+        }
+        graphs.push_back(GraphEntry{&L, dW, dY, nrhs, accumulate, exec});
+        hit = &graphs.back();
+    }
+    MXB_CUDA(cudaGraphLaunch(hit->exec, stream));
+    return MXB_OK;
+}
+
+int Plan::enqueue(const std::vector<Launch> &L, const double *dW, double *dY, int nrhs, int accumulate,
+                  cudaStream_t stream)
+{
     if (precision != MXB_PREC_FP64) return run_split_bf16(L, dW, dY, nrhs, accumulate, stream);
     Operands ops{};
     ops.pool[0] = dD;

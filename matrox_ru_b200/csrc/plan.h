@@ -59,8 +59,23 @@ struct Plan : public mxb_plan {
     int read_workspaces(int nrhs, const int32_t *wsko, double *wskel, const int32_t *usko, double *uskel);
     uint64_t flops(int nrhs) const;
 
+    // evaluation replay: one CUDA graph per (operands, nrhs, accumulate, direction)
+    struct GraphEntry {
+        const void *launches;
+        const double *W;
+        double *Y;
+        int nrhs, accumulate;
+        cudaGraphExec_t exec;
+    };
+    std::vector<GraphEntry> graphs;
+    cudaStream_t capture_stream = nullptr;
+    void clear_graphs();
+    int enqueue(const std::vector<Launch> &L, const double *dW, double *dY, int nrhs, int accumulate,
+                cudaStream_t stream);
+
     // split-BF16 path (split_bf16.cu)
     int setup_split_bf16(const mxb_cds_desc &d);
+    int prepare_split_bf16(int nrhs, bool *reallocated);
     int run_split_bf16(const std::vector<Launch> &L, const double *dW, double *dY, int nrhs, int accumulate,
                        cudaStream_t stream);
     void free_split_bf16();
@@ -69,6 +84,7 @@ struct Plan : public mxb_plan {
 const char *last_error();
 int row_tile_for(int precision);
 int split_bf16_launches(const Plan &p);
+int split_bf16_prepare();
 int split_bf16_status(Plan &p);
 
 }  // namespace mxb

@@ -408,8 +408,12 @@ cudaError_t launch_tc(const Task *tasks, const TcItem *items, int ntasks, const 
         e = cudaDeviceGetAttribute(&g_sm_count[dev], cudaDevAttrMultiProcessorCount, dev);
         if (e != cudaSuccess) return e;
     }
-    e = cudaFuncSetAttribute(tc_gemm_kernel<P, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
-    if (e != cudaSuccess) return e;
+    static bool configured[128];
+    if (!configured[dev]) {
+        e = cudaFuncSetAttribute(tc_gemm_kernel<P, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
+        if (e != cudaSuccess) return e;
+        configured[dev] = true;
+    }
     const int nunits = ntasks * ((a.nrhs + BN - 1) / BN);
     const int grid = std::min(nunits, g_sm_count[dev]);
     tc_gemm_kernel<P, BN><<<grid, C::THREADS, C::SMEM, s>>>(tasks, items, nunits, a);
@@ -723,6 +727,15 @@ static int split_buffers(Plan &p, SplitBF16 &S, int nrhs)
     return MXB_OK;
 }
 
+int Plan::prepare_split_bf16(int nrhs, bool *reallocated)
+{
+    const int nt_before = bf16->nt_cap, n_before = bf16->nrhs_cap;
+    int rc = split_buffers(*this, *bf16, nrhs);
+    if (rc) return rc;
+    *reallocated = bf16->nt_cap != nt_before || bf16->nrhs_cap != n_before;
+    return split_bf16_prepare();
+}
+
 int Plan::run_split_bf16(const std::vector<Launch> &L, const double *dW, double *dY, int nrhs, int accumulate,
                          cudaStream_t stream)
 {
@@ -731,8 +744,6 @@ int Plan::run_split_bf16(const std::vector<Launch> &L, const double *dW, double 
         return MXB_ERR_UNSUPPORTED;
     }
     SplitBF16 &S = *bf16;
-    int rc = split_buffers(*this, S, nrhs);
-    if (rc) return rc;
     const int NT = S.nt_cap;
     cudaError_t e = cudaSuccess;
     for (const Op &o : S.ops) {
@@ -770,6 +781,22 @@ int Plan::run_split_bf16(const std::vector<Launch> &L, const double *dW, double 
             set_error(std::string("split-BF16 launch: ") + cudaGetErrorString(e));
             return MXB_ERR_CUDA;
         }
+    }
+    return MXB_OK;
+}
+
+int split_bf16_prepare()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return MXB_ERR_CUDA;
+    if (!g_sm_count[dev] && cudaDeviceGetAttribute(&g_sm_count[dev], cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return MXB_ERR_CUDA;
+    if (cudaFuncSetAttribute(tc_gemm_kernel<2, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             TcCfg<2, 256>::SMEM) != cudaSuccess ||
+        cudaFuncSetAttribute(tc_gemm_kernel<3, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             TcCfg<3, 128>::SMEM) != cudaSuccess) {
+        set_error("configuring the tensor-core kernels' shared memory failed");
+        return MXB_ERR_CUDA;
     }
     return MXB_OK;
 }
