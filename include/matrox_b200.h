@@ -223,6 +223,14 @@ MXB_API int32_t mxb_plan_info(const mxb_plan *plan, uint64_t *device_bytes, int3
 /* Waits for the device and reports a kernel-side failure of earlier evaluations on the plan
  * (MXB_ERR_TIMEOUT when a bounded wait of a tensor-core kernel gave up); clears it. */
 MXB_API int32_t mxb_plan_status(mxb_plan *plan);
+/* Test hook for failure detection, no counterpart in the reference.  With
+ * MXB_DEBUG_STALL_ONE_WAIT, the first tensor-core launch of the next evaluations has one CTA
+ * withhold a pipeline stage, so its bounded wait runs out: the CTA gives up, frees its TMEM
+ * and mxb_plan_status() reports MXB_ERR_TIMEOUT, with the GPU context still usable.
+ * wait_cycles > 0 shortens every kernel wait limit (default ~4e9 SM cycles).  flags = 0
+ * restores normal operation.  Split-BF16 plans only. */
+#define MXB_DEBUG_STALL_ONE_WAIT 1
+MXB_API int32_t mxb_plan_set_test_hooks(mxb_plan *plan, int32_t flags, int64_t wait_cycles);
 /* Copies the last evaluation's skeleton workspaces (wskel, uskel) to host arrays laid out
  * with the caller's wskeloffset / uskeloffset (for callers that inspect them). */
 MXB_API int32_t mxb_plan_read_workspaces(mxb_plan *plan, int32_t nrhs, const int32_t *wskeloffset,

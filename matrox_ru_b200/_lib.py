@@ -25,6 +25,7 @@ PREC_SPLIT_BF16_FAR6 = 2
 PREC_SPLIT_BF16_X6 = 3
 FLAG_MIRROR_WORKSPACES = 1
 FLAG_OUTPUT_IS_ZERO = 2
+DEBUG_STALL_ONE_WAIT = 1
 
 P = ctypes.c_void_p
 I32 = ctypes.c_int32
@@ -86,6 +87,7 @@ def load(path: str = LIB_PATH):
     lib.mxb_plan_info.argtypes = [P, ctypes.POINTER(U64), ctypes.POINTER(I32), ctypes.POINTER(I32)]
     lib.mxb_plan_read_workspaces.argtypes = [P, I32, P, P, P, P]
     lib.mxb_plan_status.argtypes = [P]
+    lib.mxb_plan_set_test_hooks.argtypes = [P, I32, I64]
     lib.mxb_permute_rows.argtypes = [P, P, P, I32, I64, P, P, I64, I64, I32, I32, I32, P]
     lib.mxb_transform.argtypes = [P, P, P, I32, P, I64, I64, I32, P]
     lib.mxb_untransform.argtypes = [P, P, P, I32, P, I64, I64, I32, P]

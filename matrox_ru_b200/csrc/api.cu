@@ -771,6 +771,23 @@ int32_t mxb_plan_info(const mxb_plan *plan, uint64_t *device_bytes, int32_t *lau
     return MXB_OK;
 }
 
+int32_t mxb_plan_set_test_hooks(mxb_plan *plan, int32_t flags, int64_t wait_cycles)
+{
+    if (!plan || wait_cycles < 0) {
+        set_error("bad argument");
+        return MXB_ERR_ARG;
+    }
+    Plan *p = static_cast<Plan *>(plan);
+    if (p->precision == MXB_PREC_FP64 && flags) {
+        set_error("test hooks apply to split-BF16 plans");
+        return MXB_ERR_UNSUPPORTED;
+    }
+    p->debug_flags = flags;
+    p->debug_wait_cycles = wait_cycles;
+    p->clear_graphs();  // hooks are baked into captured graphs
+    return MXB_OK;
+}
+
 int32_t mxb_plan_status(mxb_plan *plan)
 {
     if (!plan) {

@@ -43,6 +43,8 @@ struct Plan : public mxb_plan {
     double *dWskel = nullptr, *dUskel = nullptr;
     size_t scratch_elems = 0;
     SplitBF16 *bf16 = nullptr;
+    int debug_flags = 0;              // test hooks (mxb_plan_set_test_hooks)
+    long long debug_wait_cycles = 0;  // 0: default wait limit
     std::vector<void *> allocations;
     uint64_t device_bytes = 0;
 

@@ -73,6 +73,8 @@ struct TcArgs {
     int nrhs;
     int out_kind;   // 0: FP64 Y, 1: FP32 skeleton block
     int beta_arg;
+    long long wait_cycles;  // limit of every wait in the kernel
+    int stall_test;         // test hook: CTA 0 withholds its first stage, so a wait runs out
 };
 
 // ---------------------------------------------------------------------------------------
@@ -216,6 +218,9 @@ tc_gemm_kernel(const Task *__restrict__ tasks, const TcItem *__restrict__ items,
         if (lane == 0) {
             // ---------------- producer ----------------
             uint32_t g = 0;  // global K-tile counter of this CTA
+            uint32_t filled[C::STAGES];  // rounds filled per stage (drained before exit)
+#pragma unroll
+            for (int s = 0; s < C::STAGES; ++s) filled[s] = 0;
             for (int u = blockIdx.x; u < nunits && !*abort_word; u += gridDim.x) {
                 const Task t = tasks[u / ncol];
                 const int col = u % ncol;
@@ -226,10 +231,11 @@ tc_gemm_kernel(const Task *__restrict__ tasks, const TcItem *__restrict__ items,
                     for (int kt = 0; kt < it.KT; ++kt, ++g) {
                         const int s = g % C::STAGES;
                         const uint32_t round = g / C::STAGES;
-                        if (!tc::mbar_wait(&empty[s], (round & 1) ^ 1, abort_word)) {
+                        if (!tc::mbar_wait(&empty[s], (round & 1) ^ 1, abort_word, args.wait_cycles)) {
                             *abort_word = 1;
                             break;
                         }
+                        if (args.stall_test && blockIdx.x == 0 && g == 0) continue;  // never filled
                         uint8_t *sa = smem + s * C::STAGE;
                         uint8_t *sb = sa + C::A_BYTES;
                         tc::mbar_expect_tx(&full[s], C::STAGE);
@@ -246,14 +252,16 @@ tc_gemm_kernel(const Task *__restrict__ tasks, const TcItem *__restrict__ items,
                                 tc::bulk_g2s(sb + (p * C::HALVES + hh) * TILE_BYTES, gb + (size_t)p * TILE_BYTES,
                                              TILE_BYTES, &full[s]);
                         }
+                        filled[s] = round + 1;
                     }
                 }
             }
             // every stage this thread filled must have landed before the CTA may exit
-            for (int s = 0; s < C::STAGES && (uint32_t)s < g; ++s) {
-                const uint32_t last_round = (g - 1 - s) / C::STAGES;
+#pragma unroll
+            for (int s = 0; s < C::STAGES; ++s) {
+                if (!filled[s]) continue;
                 volatile int never = 0;
-                tc::mbar_wait(&full[s], last_round & 1, &never);
+                tc::mbar_wait(&full[s], (filled[s] - 1) & 1, &never, args.wait_cycles);
             }
         }
     } else if (warp == C::EPI_WARPS + 1) {
@@ -273,8 +281,8 @@ tc_gemm_kernel(const Task *__restrict__ tasks, const TcItem *__restrict__ items,
                     const uint32_t round = g / C::STAGES;
                     const int b = g & 1;
                     const uint32_t use = g >> 1;
-                    if (!tc::mbar_wait(&acce[b], (use & 1) ^ 1, abort_word) ||
-                        !tc::mbar_wait(&full[s], round & 1, abort_word)) {
+                    if (!tc::mbar_wait(&acce[b], (use & 1) ^ 1, abort_word, args.wait_cycles) ||
+                        !tc::mbar_wait(&full[s], round & 1, abort_word, args.wait_cycles)) {
                         *abort_word = 1;
                         break;
                     }
@@ -318,7 +326,7 @@ tc_gemm_kernel(const Task *__restrict__ tasks, const TcItem *__restrict__ items,
             for (int i = 0; i < ktiles && ok; ++i, ++g) {
                 const int b = g & 1;
                 const uint32_t use = g >> 1;
-                if (!tc::mbar_wait(&accf[b], use & 1, abort_word)) {
+                if (!tc::mbar_wait(&accf[b], use & 1, abort_word, args.wait_cycles)) {
                     *abort_word = 1;
                     ok = false;
                     break;
@@ -384,7 +392,7 @@ tc_gemm_kernel(const Task *__restrict__ tasks, const TcItem *__restrict__ items,
     // all MMAs must be complete before TMEM is released (bounded, also after an abort)
     if (threadIdx.x == 0) {
         volatile int never = 0;
-        if (!tc::mbar_wait(doneb, 0, &never)) *abort_word = 1;
+        if (!tc::mbar_wait(doneb, 0, &never, args.wait_cycles)) *abort_word = 1;
     }
     __syncthreads();
     if (*abort_word && threadIdx.x == 0) atomicExch(args.err, MXB_ERR_TIMEOUT);
@@ -746,6 +754,7 @@ int Plan::run_split_bf16(const std::vector<Launch> &L, const double *dW, double 
     SplitBF16 &S = *bf16;
     const int NT = S.nt_cap;
     cudaError_t e = cudaSuccess;
+    bool first_tc = true;
     for (const Op &o : S.ops) {
         switch (o.kind) {
         case OP_SPLIT_W:
@@ -771,6 +780,9 @@ int Plan::run_split_bf16(const std::vector<Launch> &L, const double *dW, double 
             // skeleton outputs: far/down write uskel, the up-sweep writes wskel
             a.skel = (o.a_pool == POOL_VU3) ? S.w32 : S.u32;
             a.beta_arg = accumulate ? 1 : 0;
+            a.wait_cycles = debug_wait_cycles > 0 ? debug_wait_cycles : tc::WAIT_CYCLES;
+            a.stall_test = (debug_flags & MXB_DEBUG_STALL_ONE_WAIT) && first_tc;
+            first_tc = false;
             if (o.kind == OP_TC2) e = launch_tc<2, 256>(S.dTasks + o.first, S.dItems, o.count, a, stream);
             else e = launch_tc<3, 128>(S.dTasks + o.first, S.dItems, o.count, a, stream);
             break;

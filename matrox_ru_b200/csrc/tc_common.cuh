@@ -59,13 +59,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 
-// Bounded wait on `parity`; gives up when the CTA's abort word is set or the time runs out.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort_word)
+// Bounded wait on `parity`; gives up when the CTA's abort word is set or `limit` cycles pass.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort_word,
+                                          long long limit = WAIT_CYCLES)
 {
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity)) {
         if (*abort_word) return false;
-        if (clock64() - t0 > WAIT_CYCLES) return false;
+        if (clock64() - t0 > limit) return false;
     }
     return true;
 }

@@ -231,6 +231,10 @@ class Plan:
         check(_lib.load().mxb_plan_info(self._h, ctypes.byref(b), ctypes.byref(l), ctypes.byref(p)), "mxb_plan_info")
         return {"device_bytes": int(b.value), "launches": int(l.value), "precision": int(p.value)}
 
+    def set_test_hooks(self, flags: int, wait_cycles: int = 0) -> None:
+        """Failure-detection test hook (see mxb_plan_set_test_hooks)."""
+        check(_lib.load().mxb_plan_set_test_hooks(self._h, flags, wait_cycles), "mxb_plan_set_test_hooks")
+
     def status(self) -> None:
         """Synchronise and raise if a kernel of an earlier evaluation reported a failure."""
         check(_lib.load().mxb_plan_status(self._h), "mxb_plan_status")
