@@ -62,16 +62,35 @@ struct PoolJob {      // one CDS matrix -> tiled parts (plan creation)
     int32_t src_pool, ld, R, K, RT, KT, trans, parts;
 };
 
+// Output of a tensor-core task.
+enum OutKind : int16_t {
+    OUT_Y = 0,      // FP64 Y block (leaf-blocked, caller's offsets)
+    OUT_F32 = 1,    // FP32 skeleton block (a far result the down launch adds to)
+    OUT_TILES = 2,  // skeleton block written as 3-part bf16 operand tiles for the next launches
+};
+
+struct TcTask {
+    int64_t c_row;   // leaf index (OUT_Y) or skeleton row offset (FP32 block)
+    int64_t out_kt;  // K-tile base of the node in the tile buffer (OUT_TILES)
+    int32_t ldc;
+    int32_t M;       // rows of the whole output block
+    int32_t m0;      // first row of this task's 128-row tile
+    int32_t item0;
+    int32_t nitem;
+    int16_t out_kind;
+    int16_t beta;    // 0 overwrite, 1 accumulate (OUT_TILES: add the FP32 block), 2 launch arg
+};
+
 struct TcArgs {
     const uint8_t *a_pool;
     const uint8_t *b_pool;
+    uint8_t *t_pool;  // tile buffer of OUT_TILES tasks
     double *Y;
     const int32_t *yofs;
-    float *skel;
+    float *skel;      // FP32 skeleton blocks (written by OUT_F32, added by OUT_TILES with beta)
     int *err;
     int NT;         // 128-column tiles per node in the B buffers (even)
     int nrhs;
-    int out_kind;   // 0: FP64 Y, 1: FP32 skeleton block
     int beta_arg;
     long long wait_cycles;  // limit of every wait in the kernel
     int stall_test;         // test hook: CTA 0 withholds its first stage, so a wait runs out
@@ -152,6 +171,25 @@ __global__ void __launch_bounds__(256) split_b_kernel(const SplitJob *__restrict
 // tcgen05 grouped GEMM
 // ---------------------------------------------------------------------------------------
 
+// 8 x 8 transpose inside each group of 8 lanes: lane 8g + i ends with x[j] = the value lane
+// 8g + j held in x[i] (three butterfly stages of block swaps).
+__device__ __forceinline__ void transpose8(float (&x)[8], int lane)
+{
+#pragma unroll
+    for (int s = 1; s < 8; s <<= 1) {
+        const bool up = (lane & s) != 0;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            if ((i & s) == 0) {
+                const float send = up ? x[i] : x[i + s];
+                const float recv = __shfl_xor_sync(0xffffffffu, send, s);
+                if (up) x[i] = recv;
+                else x[i + s] = recv;
+            }
+        }
+    }
+}
+
 template <int P, int BN>
 struct TcCfg {
     static constexpr int STAGES = 2;
@@ -179,7 +217,7 @@ struct TcCfg {
 // and the epilogue of one unit overlaps the MMAs of the next.
 template <int P, int BN>
 __global__ void __launch_bounds__(TcCfg<P, BN>::THREADS, 1)
-tc_gemm_kernel(const Task *__restrict__ tasks, const TcItem *__restrict__ items, int nunits, TcArgs args)
+tc_gemm_kernel(const TcTask *__restrict__ tasks, const TcItem *__restrict__ items, int nunits, TcArgs args)
 {
     using C = TcCfg<P, BN>;
     extern __shared__ uint8_t smem_raw[];
@@ -222,7 +260,7 @@ tc_gemm_kernel(const Task *__restrict__ tasks, const TcItem *__restrict__ items,
 #pragma unroll
             for (int s = 0; s < C::STAGES; ++s) filled[s] = 0;
             for (int u = blockIdx.x; u < nunits && !*abort_word; u += gridDim.x) {
-                const Task t = tasks[u / ncol];
+                const TcTask t = tasks[u / ncol];
                 const int col = u % ncol;
                 const TcItem *ti = items + t.item0;
                 const int mt = t.m0 / 128;
@@ -273,7 +311,7 @@ tc_gemm_kernel(const Task *__restrict__ tasks, const TcItem *__restrict__ items,
             uint32_t g = 0;
             bool any = false;
             for (int u = blockIdx.x; u < nunits && !*abort_word; u += gridDim.x) {
-                const Task t = tasks[u / ncol];
+                const TcTask t = tasks[u / ncol];
                 int ktiles = 0;
                 for (int q = 0; q < t.nitem; ++q) ktiles += items[t.item0 + q].KT;
                 for (int i = 0; i < ktiles; ++i, ++g) {
@@ -315,7 +353,7 @@ tc_gemm_kernel(const Task *__restrict__ tasks, const TcItem *__restrict__ items,
         const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
         uint32_t g = 0;
         for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
-            const Task t = tasks[u / ncol];
+            const TcTask t = tasks[u / ncol];
             const int col = u % ncol;
             int ktiles = 0;
             for (int q = 0; q < t.nitem; ++q) ktiles += items[t.item0 + q].KT;
@@ -346,12 +384,12 @@ tc_gemm_kernel(const Task *__restrict__ tasks, const TcItem *__restrict__ items,
             }
             if (!ok || *abort_word) break;
             const int r = t.m0 + quarter * 32 + lane;
-            if (r < t.M) {
-                const int beta = t.beta == 2 ? args.beta_arg : t.beta;
-                const int col0 = col * BN + half * C::COLS;
-                // accumulating outputs: all old values of a 16-column chunk are loaded before
-                // any store, so the loads overlap instead of waiting on each other
-                if (args.out_kind == 0) {
+            const int beta = t.beta == 2 ? args.beta_arg : t.beta;
+            const int col0 = col * BN + half * C::COLS;
+            // accumulating outputs: all old values of a 16-column chunk are loaded before any
+            // store, so the loads overlap instead of waiting on each other
+            if (t.out_kind == OUT_Y) {
+                if (r < t.M) {
                     double *Yb = args.Y + args.yofs[t.c_row] + r;
 #pragma unroll
                     for (int c0 = 0; c0 < C::COLS; c0 += 16) {
@@ -367,21 +405,55 @@ tc_gemm_kernel(const Task *__restrict__ tasks, const TcItem *__restrict__ items,
                             if (cc < args.nrhs) Yb[(size_t)cc * t.ldc] = old[e] + (double)acc[c0 + e];
                         }
                     }
-                } else {
+                }
+            } else if (t.out_kind == OUT_F32) {
+                if (r < t.M) {
                     float *Sb = args.skel + t.c_row * (int64_t)args.nrhs + r;
+#pragma unroll
+                    for (int e = 0; e < C::COLS; ++e) {
+                        const int cc = col0 + e;
+                        if (cc < args.nrhs) Sb[(size_t)cc * t.ldc] = acc[e];
+                    }
+                }
+            } else {
+                // OUT_TILES: (optionally) add the FP32 far result, then write this row's values
+                // as 3-part bf16 operand tiles.  The lane holds one K index; a transpose in
+                // groups of 8 lanes gives it 8 consecutive K of one column: one 16-byte chunk
+                // per part.  Rows past M carry zeros (A is zero-padded); rows past the node's
+                // K tiles are not written.
+                if (beta && r < t.M) {
+                    const float *Sb = args.skel + t.c_row * (int64_t)args.nrhs + r;
 #pragma unroll
                     for (int c0 = 0; c0 < C::COLS; c0 += 16) {
                         float old[16];
 #pragma unroll
                         for (int e = 0; e < 16; ++e) {
                             const int cc = col0 + c0 + e;
-                            old[e] = (beta && cc < args.nrhs) ? Sb[(size_t)cc * t.ldc] : 0.f;
+                            old[e] = cc < args.nrhs ? Sb[(size_t)cc * t.ldc] : 0.f;
                         }
 #pragma unroll
-                        for (int e = 0; e < 16; ++e) {
-                            const int cc = col0 + c0 + e;
-                            if (cc < args.nrhs) Sb[(size_t)cc * t.ldc] = old[e] + acc[c0 + e];
-                        }
+                        for (int e = 0; e < 16; ++e) acc[c0 + e] += old[e];
+                    }
+                }
+                const int KTv = (t.M + 63) / 64;
+                const int k0 = t.m0 + quarter * 32 + (lane & ~7);
+                const bool k_ok = k0 < KTv * 64;
+                const int kt = k0 >> 6;
+                const uint32_t kin = (uint32_t)(k0 & 63);
+#pragma unroll
+                for (int g8 = 0; g8 < C::COLS / 8; ++g8) {
+                    float x[8];
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) x[j] = acc[8 * g8 + j];
+                    transpose8(x, lane);
+                    const int n = col0 + 8 * g8 + (lane & 7);
+                    __nv_bfloat16 h[8], m[8], l[8];
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) tc::split3(x[j], h[j], m[j], l[j]);
+                    if (k_ok) {
+                        uint8_t *tile0 = args.t_pool +
+                                         ((size_t)t.out_kt * args.NT + (size_t)(n >> 7) * KTv + kt) * 3 * (size_t)TILE_BYTES;
+                        store_parts(tile0, 3, n & 127, (int)(kin >> 3), h, m, l);
                     }
                 }
             }
@@ -404,7 +476,7 @@ tc_gemm_kernel(const Task *__restrict__ tasks, const TcItem *__restrict__ items,
 int g_sm_count[128];
 
 template <int P, int BN>
-cudaError_t launch_tc(const Task *tasks, const TcItem *items, int ntasks, const TcArgs &a, cudaStream_t s)
+cudaError_t launch_tc(const TcTask *tasks, const TcItem *items, int ntasks, const TcArgs &a, cudaStream_t s)
 {
     if (ntasks <= 0) return cudaSuccess;
     using C = TcCfg<P, BN>;
@@ -434,7 +506,7 @@ enum BBuf { BUF_W, BUF_WSKEL, BUF_USKEL };
 
 struct Op {
     int kind, first, count, max_kt;
-    int a_pool, b_buf, out_kind;
+    int a_pool, b_buf, t_buf;  // A pool, B buffer, tile buffer written by OUT_TILES tasks
 };
 
 int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
@@ -444,19 +516,19 @@ int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 struct SplitBF16 {
     uint8_t *pool[NPOOL] = {};
     size_t pool_bytes[NPOOL] = {};
-    Task *dTasks = nullptr;
+    TcTask *dTasks = nullptr;
     TcItem *dItems = nullptr;
     SplitJob *dJobs = nullptr;
     int *dErr = nullptr;
     std::vector<Op> ops;
-    std::vector<Task> tasks;
+    std::vector<TcTask> tasks;
     std::vector<TcItem> items;
     std::vector<SplitJob> jobs;
     std::vector<int64_t> leaf_kt, node_kt;  // K-tile bases
     int64_t leaf_kt_total = 0, node_kt_total = 0;
     int nt_cap = 0, nrhs_cap = 0;
     uint8_t *Wt = nullptr, *wT = nullptr, *uT = nullptr;
-    float *w32 = nullptr, *u32 = nullptr;
+    float *u32 = nullptr;  // FP32 far results awaiting the down launch
 };
 
 int Plan::setup_split_bf16(const mxb_cds_desc &)
@@ -556,12 +628,12 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
         maxh = std::max(maxh, height[v]);
         maxd = std::max(maxd, depth[v]);
     }
-    auto begin_op = [&](int kind, int a_pool, int b_buf, int out_kind) {
+    auto begin_op = [&](int kind, int a_pool, int b_buf, int t_buf) {
         Op o{};
         o.kind = kind;
         o.a_pool = a_pool;
         o.b_buf = b_buf;
-        o.out_kind = out_kind;
+        o.t_buf = t_buf;
         o.first = (kind <= OP_SPLIT_USKEL) ? (int)S->jobs.size() : (int)S->tasks.size();
         S->ops.push_back(o);
     };
@@ -569,13 +641,13 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
         Op &o = S->ops.back();
         if (o.kind >= OP_TC2) {
             // longest tasks first: balances the persistent kernel's static round-robin
-            auto cost = [&](const Task &t) {
+            auto cost = [&](const TcTask &t) {
                 int k = 0;
                 for (int q = 0; q < t.nitem; ++q) k += S->items[t.item0 + q].KT;
                 return k;
             };
             std::stable_sort(S->tasks.begin() + o.first, S->tasks.end(),
-                             [&](const Task &a, const Task &b) { return cost(a) > cost(b); });
+                             [&](const TcTask &a, const TcTask &b) { return cost(a) > cost(b); });
         }
         o.count = ((o.kind <= OP_SPLIT_USKEL) ? (int)S->jobs.size() : (int)S->tasks.size()) - o.first;
         o.max_kt = 1;
@@ -583,16 +655,18 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
             for (int j = o.first; j < o.first + o.count; ++j) o.max_kt = std::max(o.max_kt, S->jobs[j].KT);
         if (o.count == 0) S->ops.pop_back();
     };
-    auto add_tasks = [&](int16_t c_kind, int64_t c_row, int ldc, int M, int item0, int16_t beta) {
+    auto add_tasks = [&](int16_t out_kind, int64_t c_row, int64_t out_kt, int ldc, int M, int item0,
+                         int16_t beta) {
         for (int m0 = 0; m0 < M; m0 += 128) {
-            Task t{};
+            TcTask t{};
             t.c_row = c_row;
+            t.out_kt = out_kt;
             t.ldc = ldc;
             t.M = M;
             t.m0 = m0;
             t.item0 = item0;
             t.nitem = (int)S->items.size() - item0;
-            t.c_kind = c_kind;
+            t.out_kind = out_kind;
             t.beta = beta;
             S->tasks.push_back(t);
         }
@@ -618,9 +692,9 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
     begin_op(OP_SPLIT_W, -1, BUF_W, -1);
     for (int i = 0; i < nleaf; ++i) split_job(i, S->leaf_kt[i], Ddim[i], Ddim[i]);
     end_op();
-    // up-sweep by height
+    // up-sweep by height: the epilogue writes wskel directly as operand tiles
     for (int h = 0; h <= maxh; ++h) {
-        begin_op(OP_TC3, POOL_VU3, h == 0 ? BUF_W : BUF_WSKEL, 1);
+        begin_op(OP_TC3, POOL_VU3, h == 0 ? BUF_W : BUF_WSKEL, BUF_WSKEL);
         for (int v : bfs) {
             if (height[v] != h || !projects(v)) continue;
             const int item0 = (int)S->items.size();
@@ -630,71 +704,62 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
                 if (slen[lch[v]] > 0) item(up_a[v], S->node_kt[lch[v]], slen[lch[v]]);
                 if (slen[rch[v]] > 0) item(up_b[v], S->node_kt[rch[v]], slen[rch[v]]);
             }
-            add_tasks(KIND_WSKEL, skel_row[v], slen[v], slen[v], item0, 0);
+            add_tasks(OUT_TILES, skel_row[v], S->node_kt[v], slen[v], slen[v], item0, 0);
         }
         end_op();
-        begin_op(OP_SPLIT_WSKEL, -1, BUF_WSKEL, -1);
-        for (int v : bfs)
-            if (height[v] == h && projects(v)) split_job(skel_row[v], S->node_kt[v], slen[v], slen[v]);
-        end_op();
     }
-    // far + down by depth
+    // far + down by depth: a node whose parent projects keeps its far result in FP32 for the
+    // down launch, which adds its own product and writes uskel tiles; other nodes' far
+    // results become tiles directly
+    auto has_down = [&](int c) { return parent[c] >= 0 && projects(parent[c]); };
     std::vector<std::vector<int>> far_out(numnodes);
     for (size_t k = 0; k < far_x.size(); ++k) far_out[far_x[k]].push_back((int)k);
     for (int dd = 1; dd <= maxd; ++dd) {
-        begin_op(far_parts == 2 ? OP_TC2 : OP_TC3, POOL_FAR, BUF_WSKEL, 1);
+        begin_op(far_parts == 2 ? OP_TC2 : OP_TC3, POOL_FAR, BUF_WSKEL, BUF_USKEL);
         for (int c : bfs) {
             if (depth[c] != dd || !projects(c)) continue;
             const int item0 = (int)S->items.size();
             for (int k : far_out[c])
                 if (slen[far_y[k]] > 0) item(far_a[k], S->node_kt[far_y[k]], slen[far_y[k]]);
-            add_tasks(KIND_USKEL, skel_row[c], slen[c], slen[c], item0, 0);
+            add_tasks(has_down(c) ? OUT_F32 : OUT_TILES, skel_row[c], S->node_kt[c], slen[c], slen[c], item0, 0);
         }
         end_op();
-        begin_op(OP_TC3, POOL_VD3, BUF_USKEL, 1);
+        begin_op(OP_TC3, POOL_VD3, BUF_USKEL, BUF_USKEL);
         for (int c : bfs) {
-            if (depth[c] != dd || !projects(c)) continue;
-            const int p = parent[c];
-            if (p < 0 || !projects(p)) continue;
+            if (depth[c] != dd || !projects(c) || !has_down(c)) continue;
             const int item0 = (int)S->items.size();
-            item(down_child[c], S->node_kt[p], slen[p]);
-            add_tasks(KIND_USKEL, skel_row[c], slen[c], slen[c], item0, 1);
+            item(down_child[c], S->node_kt[parent[c]], slen[parent[c]]);
+            add_tasks(OUT_TILES, skel_row[c], S->node_kt[c], slen[c], slen[c], item0, 1);
         }
-        end_op();
-        begin_op(OP_SPLIT_USKEL, -1, BUF_USKEL, -1);
-        for (int c : bfs)
-            if (depth[c] == dd && projects(c) && lch[c] != -1) split_job(skel_row[c], S->node_kt[c], slen[c], slen[c]);
-        for (int c : bfs)  // leaves' uskel feeds the leaf-down launch
-            if (depth[c] == dd && projects(c) && lch[c] == -1) split_job(skel_row[c], S->node_kt[c], slen[c], slen[c]);
         end_op();
     }
     // near (Y (+)= D W) then leaf down (Y += P^T uskel)
     std::vector<std::vector<int>> near_out(nleaf);
     for (size_t k = 0; k < near_x.size(); ++k) near_out[near_x[k]].push_back((int)k);
-    begin_op(near_parts == 2 ? OP_TC2 : OP_TC3, POOL_NEAR, BUF_W, 0);
+    begin_op(near_parts == 2 ? OP_TC2 : OP_TC3, POOL_NEAR, BUF_W, -1);
     for (int v : bfs) {
         if (lch[v] != -1) continue;
         const int x = lm[v];
         const int item0 = (int)S->items.size();
         for (int k : near_out[x]) item(near_a[k], S->leaf_kt[near_y[k]], Ddim[near_y[k]]);
-        add_tasks(KIND_Y, x, Ddim[x], Ddim[x], item0, 2);
+        add_tasks(OUT_Y, x, 0, Ddim[x], Ddim[x], item0, 2);
     }
     end_op();
-    begin_op(OP_TC3, POOL_VD3, BUF_USKEL, 0);
+    begin_op(OP_TC3, POOL_VD3, BUF_USKEL, -1);
     for (int v : bfs) {
         if (lch[v] != -1 || !projects(v)) continue;
         const int item0 = (int)S->items.size();
         item(down_a[v], S->node_kt[v], slen[v]);
-        add_tasks(KIND_Y, lm[v], Ddim[lm[v]], Ddim[lm[v]], item0, 1);
+        add_tasks(OUT_Y, lm[v], 0, Ddim[lm[v]], Ddim[lm[v]], item0, 1);
     }
     end_op();
 
-    int rc = alloc((void **)&S->dTasks, std::max<size_t>(S->tasks.size(), 1) * sizeof(Task));
+    int rc = alloc((void **)&S->dTasks, std::max<size_t>(S->tasks.size(), 1) * sizeof(TcTask));
     if (!rc) rc = alloc((void **)&S->dItems, std::max<size_t>(S->items.size(), 1) * sizeof(TcItem));
     if (!rc) rc = alloc((void **)&S->dJobs, std::max<size_t>(S->jobs.size(), 1) * sizeof(SplitJob));
     if (!rc) rc = alloc((void **)&S->dErr, sizeof(int));
     if (rc) return rc;
-    cudaError_t e = cudaMemcpy(S->dTasks, S->tasks.data(), S->tasks.size() * sizeof(Task), cudaMemcpyHostToDevice);
+    cudaError_t e = cudaMemcpy(S->dTasks, S->tasks.data(), S->tasks.size() * sizeof(TcTask), cudaMemcpyHostToDevice);
     if (e == cudaSuccess && !S->items.empty())
         e = cudaMemcpy(S->dItems, S->items.data(), S->items.size() * sizeof(TcItem), cudaMemcpyHostToDevice);
     if (e == cudaSuccess && !S->jobs.empty())
@@ -719,15 +784,13 @@ static int split_buffers(Plan &p, SplitBF16 &S, int nrhs)
     release(S.Wt);
     release(S.wT);
     release(S.uT);
-    release(S.w32);
     release(S.u32);
     S.Wt = S.wT = S.uT = nullptr;
-    S.w32 = S.u32 = nullptr;
+    S.u32 = nullptr;
     const size_t tile3 = 3 * (size_t)TILE_BYTES;
     int rc = p.alloc((void **)&S.Wt, std::max<int64_t>(S.leaf_kt_total, 1) * NT * tile3);
     if (!rc) rc = p.alloc((void **)&S.wT, std::max<int64_t>(S.node_kt_total, 1) * NT * tile3);
     if (!rc) rc = p.alloc((void **)&S.uT, std::max<int64_t>(S.node_kt_total, 1) * NT * tile3);
-    if (!rc) rc = p.alloc((void **)&S.w32, std::max<int64_t>(p.skel_total, 1) * (size_t)nrhs * sizeof(float));
     if (!rc) rc = p.alloc((void **)&S.u32, std::max<int64_t>(p.skel_total, 1) * (size_t)nrhs * sizeof(float));
     if (rc) return rc;
     S.nt_cap = NT;
@@ -761,24 +824,17 @@ int Plan::run_split_bf16(const std::vector<Launch> &L, const double *dW, double 
             split_b_kernel<double><<<dim3(o.count, o.max_kt, NT), 256, 0, stream>>>(S.dJobs + o.first, dW, dOfs,
                                                                                   nrhs, NT, S.Wt);
             break;
-        case OP_SPLIT_WSKEL:
-        case OP_SPLIT_USKEL:
-            split_b_kernel<float><<<dim3(o.count, o.max_kt, NT), 256, 0, stream>>>(
-                S.dJobs + o.first, o.kind == OP_SPLIT_WSKEL ? S.w32 : S.u32, nullptr, nrhs, NT,
-                o.kind == OP_SPLIT_WSKEL ? S.wT : S.uT);
-            break;
         default: {
             TcArgs a{};
             a.a_pool = S.pool[o.a_pool];
             a.b_pool = o.b_buf == BUF_W ? S.Wt : (o.b_buf == BUF_WSKEL ? S.wT : S.uT);
+            a.t_pool = o.t_buf == BUF_WSKEL ? S.wT : S.uT;
             a.Y = dY;
             a.yofs = dOfs + nleaf;
             a.err = S.dErr;
             a.NT = NT;
             a.nrhs = nrhs;
-            a.out_kind = o.out_kind == 0 ? 0 : 1;
-            // skeleton outputs: far/down write uskel, the up-sweep writes wskel
-            a.skel = (o.a_pool == POOL_VU3) ? S.w32 : S.u32;
+            a.skel = S.u32;
             a.beta_arg = accumulate ? 1 : 0;
             a.wait_cycles = debug_wait_cycles > 0 ? debug_wait_cycles : tc::WAIT_CYCLES;
             a.stall_test = (debug_flags & MXB_DEBUG_STALL_ONE_WAIT) && first_tc;
