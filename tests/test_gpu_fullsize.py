@@ -1,0 +1,77 @@
+"""GPU: the full c1 workload (H2-b, N=65536, d=28, 1024 rhs) through size-independent
+properties and a column slice of the reference's own evaluator."""
+import numpy as np
+import pytest
+
+import oracle as O
+from matrox_ru_b200 import hgemm as H, structure as S
+
+pytestmark = pytest.mark.gpu
+SEED = 20261203
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as t
+    assert t.cuda.is_available(), "GPU tests need a CUDA device"
+    from matrox_ru_b200 import build
+    build.build()
+    return t
+
+
+@pytest.fixture(scope="module")
+def c1():
+    X = S.gaussian_mixture(65536, 28, 16, -2.0, 2.0, 0.3, 1.0, seed=SEED)
+    return S.build_cds(X, S.KernelSpec("gaussian", 2.0), leaf_size=256, budget=0.03, tol=1e-5,
+                       max_rank=256, seed=SEED)
+
+
+def leaf_slice(cds, TW, r_full, r):
+    out = np.empty(cds.n * r)
+    for i in range(cds.nleaf):
+        a, b = int(cds.leaf_lids_offset[i]), int(cds.leaf_lids_offset[i + 1])
+        out[a * r:b * r] = TW[a * r_full:a * r_full + (b - a) * r]
+    return out
+
+
+def test_c1_structure_matches_reference_scale(c1):
+    assert (c1.nleaf, c1.ncount) == (256, 1536) and 2900 <= c1.fcount <= 3400
+    assert 8.0e11 <= c1.flops(1024) <= 9.0e11  # the reference's c1-shaped probe: 8.12e11
+
+
+def test_c1_fp64_reference_slice_linearity_and_adjoint(torch, c1):
+    r = 1024
+    rng = np.random.default_rng(1)
+    W1 = torch.as_tensor(rng.standard_normal(c1.n * r), device="cuda")
+    W2 = torch.as_tensor(rng.standard_normal(c1.n * r), device="cuda")
+    plan = H.Plan(c1, "fp64")
+    Y1 = plan.evaluate(W1, r)
+    Y2 = plan.evaluate(W2, r)
+    Y12 = plan.evaluate(2.0 * W1 - 0.5 * W2, r)
+    lin = (Y12 - (2.0 * Y1 - 0.5 * Y2)).abs().max().item() / Y12.abs().max().item()
+    assert lin <= 1e-12
+    # the reference's CBHGEMM on the first 8 columns of every leaf block
+    if O.ref_available():
+        rs = 8
+        tw = leaf_slice(c1, W1.cpu().numpy(), r, rs)
+        want = O.eval_h2b(c1, tw, rs, use_reference=True)
+        got = leaf_slice(c1, Y1.cpu().numpy(), r, rs)
+        assert np.abs(got - want).max() / np.abs(want).max() <= 1e-12
+    # adjoint identity <K~ W, G> = <W, K~^T G> at full size
+    G = torch.as_tensor(rng.standard_normal(c1.n * r), device="cuda")
+    A = plan.adjoint(G, r)
+    lhs = torch.dot(Y1, G).item()
+    rhs = torch.dot(W1, A).item()
+    assert abs(lhs - rhs) <= 1e-10 * abs(lhs)
+
+
+@pytest.mark.parametrize("mode,tol", [("split_bf16", 1e-5), ("split_bf16_x6", 4e-6)])
+def test_c1_split_bf16_full_columns(torch, c1, mode, tol):
+    r = 1024
+    W = torch.as_tensor(np.random.default_rng(2).standard_normal(c1.n * r), device="cuda")
+    want = H.Plan(c1, "fp64").evaluate(W, r)
+    plan = H.Plan(c1, mode)
+    got = plan.evaluate(W, r)
+    plan.status()
+    err = (torch.linalg.norm(got - want) / torch.linalg.norm(want)).item()
+    assert 1e-12 < err <= tol, err
