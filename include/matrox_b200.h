@@ -236,6 +236,26 @@ MXB_API int32_t mxb_plan_set_test_hooks(mxb_plan *plan, int32_t flags, int64_t w
 MXB_API int32_t mxb_plan_read_workspaces(mxb_plan *plan, int32_t nrhs, const int32_t *wskeloffset,
                                  double *wskel, const int32_t *uskeloffset, double *uskel);
 
+/* ---- batches: many H-matrices in one launch sequence ---------------------------------------- */
+
+/* No counterpart in the reference (which evaluates one matrix per HGEMM call).  A batch merges
+ * the launch sequences of several split-BF16 plans (same precision mode, same device; uneven
+ * N, ranks and nrhs allowed): one tensor-core launch per level serves every plan, the whole
+ * evaluation is captured as one CUDA graph, and the column-tile width of every launch is
+ * picked by timing the candidates (64 / 128 / 256 right-hand sides) on the first evaluation of
+ * an nrhs signature (MXB_AUTOTUNE=0 disables the measurement).  The plans must outlive the
+ * batch; dW[i] / dY[i] are packed leaf-blocked device arrays of plan i with nrhs[i] columns. */
+typedef struct mxb_batch mxb_batch;
+MXB_API int32_t mxb_batch_create(mxb_plan *const *plans, int32_t count, mxb_batch **out);
+MXB_API int32_t mxb_batch_evaluate(mxb_batch *batch, const double *const *dW, double *const *dY,
+                                   const int32_t *nrhs, int32_t accumulate, void *stream);
+/* Synchronises and reports a kernel-side failure (MXB_ERR_TIMEOUT) of any plan; clears it. */
+MXB_API int32_t mxb_batch_status(mxb_batch *batch);
+/* Launches per evaluation and the tuned column-tile widths of the last evaluation. */
+MXB_API int32_t mxb_batch_info(const mxb_batch *batch, int32_t *launches, int32_t *widths, int32_t cap,
+                               int32_t *nwidths);
+MXB_API int32_t mxb_batch_destroy(mxb_batch *batch);
+
 /* ---- evaluation without device allocation ------------------------------------------------ */
 
 /* No counterpart in the reference (its evaluator runs on the host).  For callers that may

@@ -87,6 +87,11 @@ def load(path: str = LIB_PATH):
     lib.mxb_plan_info.argtypes = [P, ctypes.POINTER(U64), ctypes.POINTER(I32), ctypes.POINTER(I32)]
     lib.mxb_plan_read_workspaces.argtypes = [P, I32, P, P, P, P]
     lib.mxb_plan_status.argtypes = [P]
+    lib.mxb_batch_create.argtypes = [ctypes.POINTER(P), I32, ctypes.POINTER(P)]
+    lib.mxb_batch_evaluate.argtypes = [P, ctypes.POINTER(P), ctypes.POINTER(P), ctypes.POINTER(I32), I32, P]
+    lib.mxb_batch_status.argtypes = [P]
+    lib.mxb_batch_info.argtypes = [P, ctypes.POINTER(I32), ctypes.POINTER(I32), I32, ctypes.POINTER(I32)]
+    lib.mxb_batch_destroy.argtypes = [P]
     lib.mxb_plan_set_test_hooks.argtypes = [P, I32, I64]
     lib.mxb_permute_rows.argtypes = [P, P, P, I32, I64, P, P, I64, I64, I32, I32, I32, P]
     lib.mxb_transform.argtypes = [P, P, P, I32, P, I64, I64, I32, P]

@@ -771,6 +771,54 @@ int32_t mxb_plan_info(const mxb_plan *plan, uint64_t *device_bytes, int32_t *lau
     return MXB_OK;
 }
 
+int32_t mxb_batch_create(mxb_plan *const *plans, int32_t count, mxb_batch **out)
+{
+    if (!plans || count < 1 || !out) {
+        set_error("mxb_batch_create: bad argument");
+        return MXB_ERR_ARG;
+    }
+    std::vector<Plan *> ps(count);
+    for (int i = 0; i < count; ++i) {
+        ps[i] = static_cast<Plan *>(plans[i]);
+        if (!ps[i]) {
+            set_error("mxb_batch_create: null plan");
+            return MXB_ERR_ARG;
+        }
+    }
+    Batch *b = nullptr;
+    int rc = batch_create(ps.data(), count, &b);
+    if (rc) return rc;
+    *out = reinterpret_cast<mxb_batch *>(static_cast<mxb_batch *>(reinterpret_cast<mxb_batch *>(b)));
+    return MXB_OK;
+}
+
+int32_t mxb_batch_evaluate(mxb_batch *batch, const double *const *dW, double *const *dY, const int32_t *nrhs,
+                           int32_t accumulate, void *stream)
+{
+    return batch_evaluate(reinterpret_cast<Batch *>(batch), dW, dY, nrhs, accumulate, (cudaStream_t)stream);
+}
+
+int32_t mxb_batch_status(mxb_batch *batch) { return batch_status(reinterpret_cast<Batch *>(batch)); }
+
+int32_t mxb_batch_info(const mxb_batch *batch, int32_t *launches, int32_t *widths, int32_t cap, int32_t *nwidths)
+{
+    if (!batch) {
+        set_error("null batch");
+        return MXB_ERR_ARG;
+    }
+    const Batch *b = reinterpret_cast<const Batch *>(batch);
+    if (launches) *launches = batch_launches(b);
+    const int n = widths && cap > 0 ? batch_tuned_widths(b, widths, cap) : 0;
+    if (nwidths) *nwidths = n;
+    return MXB_OK;
+}
+
+int32_t mxb_batch_destroy(mxb_batch *batch)
+{
+    batch_destroy(reinterpret_cast<Batch *>(batch));
+    return MXB_OK;
+}
+
 int32_t mxb_plan_set_test_hooks(mxb_plan *plan, int32_t flags, int64_t wait_cycles)
 {
     if (!plan || wait_cycles < 0) {

@@ -414,6 +414,7 @@ void Plan::clear_graphs()
 {
     for (GraphEntry &g : graphs) cudaGraphExecDestroy(g.exec);
     graphs.clear();
+    clear_split_graphs();
 }
 
 int Plan::ensure_scratch(int nrhs)
@@ -486,14 +487,8 @@ int Plan::run(const std::vector<Launch> &L, const double *dW, double *dY, int nr
     if (rc) return rc;
     rc = stage_offsets(1, yofs, nrhs, stream);
     if (rc) return rc;
-    if (precision != MXB_PREC_FP64) {
-        bool realloc = false;
-        rc = prepare_split_bf16(nrhs, &realloc);
-        if (rc) return rc;
-        if (realloc) clear_graphs();
-    } else {
-        MXB_CUDA(prepare_gemm_f64());
-    }
+    if (precision != MXB_PREC_FP64) return run_split_bf16(L, dW, dY, nrhs, accumulate, stream);
+    MXB_CUDA(prepare_gemm_f64());
     static const bool use_graphs = [] {
         const char *e = getenv("MXB_NO_GRAPHS");
         return !(e && *e && *e != '0');

@@ -9,10 +9,14 @@
 struct mxb_plan {
     virtual ~mxb_plan() = default;
 };
+struct mxb_batch {
+    virtual ~mxb_batch() = default;
+};
 
 namespace mxb {
 
 struct SplitBF16;  // device state of the split-BF16 path (split_bf16.cu)
+struct Batch;     // merged launch sequence of several split-BF16 plans (split_bf16.cu)
 
 struct Plan : public mxb_plan {
     ~Plan() override;
@@ -77,7 +81,7 @@ struct Plan : public mxb_plan {
 
     // split-BF16 path (split_bf16.cu)
     int setup_split_bf16(const mxb_cds_desc &d);
-    int prepare_split_bf16(int nrhs, bool *reallocated);
+    void clear_split_graphs();
     int run_split_bf16(const std::vector<Launch> &L, const double *dW, double *dY, int nrhs, int accumulate,
                        cudaStream_t stream);
     void free_split_bf16();
@@ -87,6 +91,13 @@ const char *last_error();
 int row_tile_for(int precision);
 int split_bf16_launches(const Plan &p);
 int split_bf16_prepare();
+int batch_create(Plan *const *plans, int count, Batch **out);
+int batch_evaluate(Batch *b, const double *const *W, double *const *Y, const int *nrhs, int accumulate,
+                   cudaStream_t stream);
+int batch_status(Batch *b);
+void batch_destroy(Batch *b);
+int batch_launches(const Batch *b);
+int batch_tuned_widths(const Batch *b, int *widths, int cap);
 int split_bf16_status(Plan &p);
 
 }  // namespace mxb

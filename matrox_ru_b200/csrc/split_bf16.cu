@@ -1,32 +1,37 @@
 // Split-BF16 evaluation path on the 5th-generation tensor cores (tcgen05).
 //
-// Precision scheme (per north-star: BF16 tensor-core products with split operands, FP32
-// accumulation, FP32-accurate transfers, FP64 final Y):
+// Precision scheme (BF16 tensor-core products with split operands, FP32 accumulation,
+// FP32-accurate transfers, FP64 final Y):
 //   near D_xy W_y and far B_xy wskel_y : both operands split into bf16 hi + mid, three
-//        products hi*hi + hi*mid + mid*hi ("bf16x3"), FP32 accumulation in TMEM.  Splitting
-//        only W leaves the CDS operand at 8 bits (~2e-3 relative error); splitting both
-//        gives ~5e-6.
+//        products hi*hi + hi*mid + mid*hi ("bf16x3"), FP32 accumulation.  Splitting only W
+//        leaves the CDS operand at 8 bits (~2e-3 relative error); splitting both gives ~5e-6.
 //   transfers (leaf / internal projections up and down): hi + mid + lo (24 bits), six
 //        products ("bf16x6"), which matches an FP32 SGEMM's error (~3e-7).
 //   Y: FP64, accumulated from the FP32 tile in the epilogue.
 //
 // Data layout: every operand lives in HBM already in the shared-memory tile format
-// (128 rows x 64 K bf16, K-major, 128-byte swizzle; parts of one tile contiguous), so each
+// (128 rows x 64 K bf16, K-major, 128-byte swizzle; the parts of one tile contiguous), so a
 // pipeline stage is filled by a few 1-D bulk copies (cp.async.bulk) on an mbarrier -- no
 // tensor maps, no per-element address math in the main loop.  The CDS operands (D, B, the
-// projections and their transposes) are tiled once when the plan is created; W and the
-// skeleton vectors are tiled per evaluation by split kernels (HBM-bound passes).
+// projections and their transposes) are tiled once when the plan is created; W is tiled per
+// evaluation by a split kernel, and the skeleton vectors are written as tiles directly by the
+// GEMM epilogue.
 //
-// GEMM kernel: one CTA per (task row tile, 128|256 right-hand sides), 10 warps:
+// GEMM kernel (persistent, one CTA per SM, 10 warps), walking a list of work units
+// (task row tile x BN right-hand sides; BN = 64, 128 or 256, picked by the autotuner):
 //   warp 8 lane 0 : producer -- bulk copies of the A and B part tiles of each K step
-//   warp 9 lane 0 : MMA issuer -- tcgen05.mma M=128, N=BN, K=16, 3 or 6 per 16-K slice,
-//                   one fresh TMEM accumulator (of two) per 64-deep K tile
+//   warp 9 lane 0 : MMA issuer -- tcgen05.mma M=128, N=BN, K=16, 3 or 6 per 16-K slice, one
+//                   fresh TMEM accumulator (of two) per 64-deep K tile
 //   warps 0-7     : drain every K tile's accumulator into round-to-nearest FP32 registers
-//                   (tcgen05.ld), then store rows with coalesced writes
-// Every wait is bounded (tc::WAIT_CYCLES); a CTA that times out raises MXB_ERR_TIMEOUT in
-// the plan's error word, drains its own copies and MMAs, frees its TMEM and exits.
+//                   (tcgen05.ld), then write Y (FP64), an FP32 block, or operand tiles
+// A task carries the index of its plan, so one launch can serve many H-matrices (batches).
+// Every wait is bounded; a CTA that times out raises MXB_ERR_TIMEOUT in the error word,
+// drains its own copies and MMAs, frees its TMEM and exits.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
+#include <map>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -34,6 +39,15 @@
 #include "mxb_internal.h"
 #include "plan.h"
 #include "tc_common.cuh"
+
+#define MXB_CUDA_OR(call)                                                                 \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess) {                                                          \
+            set_error(std::string(#call) + ": " + cudaGetErrorString(e_));                \
+            return MXB_ERR_CUDA;                                                          \
+        }                                                                                 \
+    } while (0)
 
 namespace mxb {
 
@@ -43,23 +57,14 @@ namespace {
 
 using tc::TILE_BYTES;
 
+enum APool { POOL_NEAR, POOL_FAR, POOL_VU3, POOL_VD3, NPOOL };
+enum BBuf { BUF_W, BUF_WSKEL, BUF_USKEL, NBUF };
+
 struct TcItem {
-    uint64_t a_off;   // byte offset of A's tile (0, 0) in the launch's A pool
+    uint64_t a_off;   // byte offset of A's tile (0, 0) in the plan's A pool of the launch
     int64_t b_base;   // K-tile base of the B operand's node / leaf in the B buffer
     int32_t KT;       // K tiles of this item
     int32_t pad;
-};
-
-struct SplitJob {     // one leaf block of W or one skeleton block -> tiled parts
-    int64_t src_row;  // leaf index (W) or skeleton row offset
-    int64_t dst_kt;   // K-tile base in the destination buffer
-    int32_t ld, K, KT, pad;
-};
-
-struct PoolJob {      // one CDS matrix -> tiled parts (plan creation)
-    uint64_t src_off;  // element offset in the FP64 pool
-    uint64_t dst_off;  // byte offset of tile (0, 0)
-    int32_t src_pool, ld, R, K, RT, KT, trans, parts;
 };
 
 // Output of a tensor-core task.
@@ -77,22 +82,53 @@ struct TcTask {
     int32_t m0;      // first row of this task's 128-row tile
     int32_t item0;
     int32_t nitem;
+    int32_t plan;    // index into the launch's plan table
     int16_t out_kind;
-    int16_t beta;    // 0 overwrite, 1 accumulate (OUT_TILES: add the FP32 block), 2 launch arg
+    int16_t beta;    // 0 overwrite, 1 accumulate (OUT_TILES: add the FP32 block), 2 plan's arg
+    int32_t pad;
 };
 
-struct TcArgs {
-    const uint8_t *a_pool;
-    const uint8_t *b_pool;
-    uint8_t *t_pool;  // tile buffer of OUT_TILES tasks
+struct TcUnit {
+    int32_t task;
+    int32_t col;     // column tile: right-hand sides [col * BN, col * BN + BN)
+};
+
+struct SplitJob {     // one leaf block of W -> B-operand tiles
+    int64_t src_row;  // leaf index
+    int64_t dst_kt;   // K-tile base in the W tile buffer
+    int32_t ld, K, KT, plan;
+};
+
+struct PoolJob {      // one CDS matrix -> tiled parts (plan creation)
+    uint64_t src_off;  // element offset in the FP64 pool
+    uint64_t dst_off;  // byte offset of tile (0, 0)
+    int32_t src_pool, ld, R, K, RT, KT, trans, parts;
+};
+
+// Per-plan pointers of one evaluation (device table indexed by TcTask::plan / SplitJob::plan).
+struct PlanArgs {
+    const uint8_t *pool[NPOOL];
+    uint8_t *buf[NBUF];  // W tiles, wskel tiles, uskel tiles
+    const double *W;
     double *Y;
+    const int32_t *wofs;
     const int32_t *yofs;
-    float *skel;      // FP32 skeleton blocks (written by OUT_F32, added by OUT_TILES with beta)
+    float *skel;         // FP32 far results awaiting the down launch
+    int32_t NT;          // 128-column tiles per node in the B buffers (even)
+    int32_t nrhs;
+    int32_t beta_arg;
+    int32_t pad;
+};
+
+struct LaunchArgs {
+    const PlanArgs *plans;
+    const TcTask *tasks;
+    const TcItem *items;
+    const TcUnit *units;
     int *err;
-    int NT;         // 128-column tiles per node in the B buffers (even)
-    int nrhs;
-    int beta_arg;
     long long wait_cycles;  // limit of every wait in the kernel
+    int nunits;
+    int a_pool, b_buf, t_buf;
     int stall_test;         // test hook: CTA 0 withholds its first stage, so a wait runs out
 };
 
@@ -139,18 +175,18 @@ __global__ void __launch_bounds__(256) tile_pool_kernel(const PoolJob *__restric
     }
 }
 
-// W (FP64, leaf-blocked) or a skeleton block (FP32) -> B-operand tiles with 3 parts.
-// B(n, k) = src[k + n ld]; rows n >= nrhs and k >= K are zero.
-template <typename T>
-__global__ void __launch_bounds__(256) split_b_kernel(const SplitJob *__restrict__ jobs, const T *__restrict__ base,
-                                                      const int32_t *__restrict__ ofs, int nrhs, int NT,
-                                                      uint8_t *__restrict__ dst)
+// W (FP64, leaf-blocked) -> B-operand tiles with 3 parts, for every plan of the launch.
+// B(n, k) = W[k + n ld]; rows n >= nrhs and k >= K are zero.
+__global__ void __launch_bounds__(256) split_w_kernel(const SplitJob *__restrict__ jobs,
+                                                      const PlanArgs *__restrict__ plans)
 {
     const SplitJob j = jobs[blockIdx.x];
+    const PlanArgs *pa = plans + j.plan;
     const int kt = blockIdx.y, nt = blockIdx.z;
-    if (kt >= j.KT) return;
-    const T *src = base + (ofs ? (int64_t)ofs[j.src_row] : j.src_row * (int64_t)nrhs);
-    uint8_t *tile0 = dst + ((size_t)j.dst_kt * NT + (size_t)nt * j.KT + kt) * 3 * (size_t)TILE_BYTES;
+    if (kt >= j.KT || nt >= pa->NT) return;
+    const int nrhs = pa->nrhs;
+    const double *src = pa->W + pa->wofs[j.src_row];
+    uint8_t *tile0 = pa->buf[BUF_W] + ((size_t)j.dst_kt * pa->NT + (size_t)nt * j.KT + kt) * 3 * (size_t)TILE_BYTES;
     for (int i = 0; i < 4; ++i) {
         const int idx = threadIdx.x + i * 256;
         const int c = idx % 8, r = idx / 8;
@@ -159,7 +195,7 @@ __global__ void __launch_bounds__(256) split_b_kernel(const SplitJob *__restrict
 #pragma unroll
         for (int e = 0; e < 8; ++e) {
             const int k = kt * 64 + c * 8 + e;
-            T x = T(0);
+            double x = 0.0;
             if (n < nrhs && k < j.K) x = src[k + (size_t)n * j.ld];
             tc::split3(x, h[e], m[e], l[e]);
         }
@@ -190,12 +226,12 @@ __device__ __forceinline__ void transpose8(float (&x)[8], int lane)
     }
 }
 
-template <int P, int BN>
+template <int P, int BN, int STAGES_>
 struct TcCfg {
-    static constexpr int STAGES = 2;
-    static constexpr int HALVES = BN / 128;
+    static constexpr int STAGES = STAGES_;
+    static constexpr int B_ROWS_BYTES = BN * 128;           // one part of the B operand, BN rows
     static constexpr int A_BYTES = P * TILE_BYTES;
-    static constexpr int B_BYTES = HALVES * P * TILE_BYTES;
+    static constexpr int B_BYTES = P * B_ROWS_BYTES;
     static constexpr int STAGE = A_BYTES + B_BYTES;
     static constexpr int SMEM = STAGES * STAGE + 1024 + 256;
     static constexpr int NPROD = P == 2 ? 3 : 6;
@@ -203,6 +239,7 @@ struct TcCfg {
     static constexpr int THREADS = (EPI_WARPS + 2) * 32;
     static constexpr int COLS = BN / 2;          // accumulator columns per epilogue thread
     static constexpr int TMEM_COLS = 2 * BN;     // two accumulator buffers
+    static_assert(SMEM <= 232448, "shared memory");
 };
 
 // Tensor-core FP32 accumulation is not round-to-nearest: its error grows with the number of
@@ -211,15 +248,13 @@ struct TcCfg {
 // epilogue warps add every tile's partial sums into per-thread FP32 registers with ordinary
 // round-to-nearest adds while the tensor core already works on the next tile.
 //
-// Persistent: one CTA per SM walks the work units u = blockIdx.x, blockIdx.x + gridDim.x, ...
-// (unit = task x column tile).  The three roles walk the same sequence, so one global K-tile
-// counter drives every stage and accumulator phase; TMEM and the barriers are set up once,
-// and the epilogue of one unit overlaps the MMAs of the next.
-template <int P, int BN>
-__global__ void __launch_bounds__(TcCfg<P, BN>::THREADS, 1)
-tc_gemm_kernel(const TcTask *__restrict__ tasks, const TcItem *__restrict__ items, int nunits, TcArgs args)
+// Persistent: CTA b walks the units b, b + gridDim.x, ...  The three roles walk the same
+// sequence, so one K-tile counter drives every stage and accumulator phase; TMEM and the
+// barriers are set up once, and the epilogue of one unit overlaps the MMAs of the next.
+template <int P, int BN, int STAGES_>
+__global__ void __launch_bounds__(TcCfg<P, BN, STAGES_>::THREADS, 1) tc_gemm_kernel(LaunchArgs la)
 {
-    using C = TcCfg<P, BN>;
+    using C = TcCfg<P, BN, STAGES_>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + C::STAGES * C::STAGE);
@@ -231,7 +266,6 @@ tc_gemm_kernel(const TcTask *__restrict__ tasks, const TcItem *__restrict__ item
     volatile int *abort_word = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int ncol = (args.nrhs + BN - 1) / BN;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < C::STAGES; ++s) {
@@ -255,40 +289,57 @@ tc_gemm_kernel(const TcTask *__restrict__ tasks, const TcItem *__restrict__ item
     if (warp == C::EPI_WARPS) {
         if (lane == 0) {
             // ---------------- producer ----------------
-            uint32_t g = 0;  // global K-tile counter of this CTA
-            uint32_t filled[C::STAGES];  // rounds filled per stage (drained before exit)
+            uint32_t g = 0;               // K-tile counter of this CTA
+            uint32_t filled[C::STAGES];   // rounds filled per stage (drained before exit)
 #pragma unroll
             for (int s = 0; s < C::STAGES; ++s) filled[s] = 0;
-            for (int u = blockIdx.x; u < nunits && !*abort_word; u += gridDim.x) {
-                const TcTask t = tasks[u / ncol];
-                const int col = u % ncol;
-                const TcItem *ti = items + t.item0;
+            for (int u = blockIdx.x; u < la.nunits && !*abort_word; u += gridDim.x) {
+                const TcUnit un = la.units[u];
+                const TcTask t = la.tasks[un.task];
+                const PlanArgs *pa = la.plans + t.plan;
+                const uint8_t *a_pool = pa->pool[la.a_pool];
+                const uint8_t *b_pool = pa->buf[la.b_buf];
+                const int NT = pa->NT;
+                const int n0 = un.col * BN;
+                const TcItem *ti = la.items + t.item0;
                 const int mt = t.m0 / 128;
                 for (int q = 0; q < t.nitem && !*abort_word; ++q) {
                     const TcItem it = ti[q];
                     for (int kt = 0; kt < it.KT; ++kt, ++g) {
                         const int s = g % C::STAGES;
                         const uint32_t round = g / C::STAGES;
-                        if (!tc::mbar_wait(&empty[s], (round & 1) ^ 1, abort_word, args.wait_cycles)) {
+                        if (!tc::mbar_wait(&empty[s], (round & 1) ^ 1, abort_word, la.wait_cycles)) {
                             *abort_word = 1;
                             break;
                         }
-                        if (args.stall_test && blockIdx.x == 0 && g == 0) continue;  // never filled
+                        if (la.stall_test && blockIdx.x == 0 && g == 0) continue;  // never filled
                         uint8_t *sa = smem + s * C::STAGE;
                         uint8_t *sb = sa + C::A_BYTES;
                         tc::mbar_expect_tx(&full[s], C::STAGE);
-                        const uint8_t *ga =
-                            args.a_pool + it.a_off + ((size_t)mt * it.KT + kt) * (size_t)P * TILE_BYTES;
+                        const uint8_t *ga = a_pool + it.a_off + ((size_t)mt * it.KT + kt) * (size_t)P * TILE_BYTES;
                         tc::bulk_g2s(sa, ga, C::A_BYTES, &full[s]);
+                        if (BN >= 128) {
 #pragma unroll
-                        for (int hh = 0; hh < C::HALVES; ++hh) {
-                            const size_t nt = (size_t)col * C::HALVES + hh;
-                            const uint8_t *gb = args.b_pool +
-                                                ((size_t)it.b_base * args.NT + nt * it.KT + kt) * 3 * (size_t)TILE_BYTES;
+                            for (int hh = 0; hh < BN / 128; ++hh) {
+                                const size_t nt = (size_t)(n0 >> 7) + hh;
+                                const uint8_t *gb =
+                                    b_pool + ((size_t)it.b_base * NT + nt * it.KT + kt) * 3 * (size_t)TILE_BYTES;
+#pragma unroll
+                                for (int p = 0; p < P; ++p)
+                                    tc::bulk_g2s(sb + p * C::B_ROWS_BYTES + hh * TILE_BYTES, gb + (size_t)p * TILE_BYTES,
+                                                 TILE_BYTES, &full[s]);
+                            }
+                        } else {
+                            // BN rows starting at row n0 % 128 of a 128-row tile: contiguous, and the
+                            // swizzle phase (row % 8) is unchanged by the 64-row offset
+                            const uint8_t *gb = b_pool +
+                                                ((size_t)it.b_base * NT + (size_t)(n0 >> 7) * it.KT + kt) * 3 *
+                                                    (size_t)TILE_BYTES +
+                                                (size_t)(n0 & 127) * 128;
 #pragma unroll
                             for (int p = 0; p < P; ++p)
-                                tc::bulk_g2s(sb + (p * C::HALVES + hh) * TILE_BYTES, gb + (size_t)p * TILE_BYTES,
-                                             TILE_BYTES, &full[s]);
+                                tc::bulk_g2s(sb + p * C::B_ROWS_BYTES, gb + (size_t)p * TILE_BYTES, C::B_ROWS_BYTES,
+                                             &full[s]);
                         }
                         filled[s] = round + 1;
                     }
@@ -299,7 +350,7 @@ tc_gemm_kernel(const TcTask *__restrict__ tasks, const TcItem *__restrict__ item
             for (int s = 0; s < C::STAGES; ++s) {
                 if (!filled[s]) continue;
                 volatile int never = 0;
-                tc::mbar_wait(&full[s], (filled[s] - 1) & 1, &never, args.wait_cycles);
+                tc::mbar_wait(&full[s], (filled[s] - 1) & 1, &never, la.wait_cycles);
             }
         }
     } else if (warp == C::EPI_WARPS + 1) {
@@ -310,17 +361,17 @@ tc_gemm_kernel(const TcTask *__restrict__ tasks, const TcItem *__restrict__ item
             constexpr int PB[6] = {0, 1, 0, 2, 1, 0};
             uint32_t g = 0;
             bool any = false;
-            for (int u = blockIdx.x; u < nunits && !*abort_word; u += gridDim.x) {
-                const TcTask t = tasks[u / ncol];
+            for (int u = blockIdx.x; u < la.nunits && !*abort_word; u += gridDim.x) {
+                const TcTask t = la.tasks[la.units[u].task];
                 int ktiles = 0;
-                for (int q = 0; q < t.nitem; ++q) ktiles += items[t.item0 + q].KT;
+                for (int q = 0; q < t.nitem; ++q) ktiles += la.items[t.item0 + q].KT;
                 for (int i = 0; i < ktiles; ++i, ++g) {
                     const int s = g % C::STAGES;
                     const uint32_t round = g / C::STAGES;
                     const int b = g & 1;
                     const uint32_t use = g >> 1;
-                    if (!tc::mbar_wait(&acce[b], (use & 1) ^ 1, abort_word, args.wait_cycles) ||
-                        !tc::mbar_wait(&full[s], round & 1, abort_word, args.wait_cycles)) {
+                    if (!tc::mbar_wait(&acce[b], (use & 1) ^ 1, abort_word, la.wait_cycles) ||
+                        !tc::mbar_wait(&full[s], round & 1, abort_word, la.wait_cycles)) {
                         *abort_word = 1;
                         break;
                     }
@@ -334,7 +385,7 @@ tc_gemm_kernel(const TcTask *__restrict__ tasks, const TcItem *__restrict__ item
 #pragma unroll
                         for (int j = 0; j < C::NPROD; ++j) {
                             const uint64_t ad = tc::smem_desc_sw128(sa + PA[j] * TILE_BYTES + ks * 32);
-                            const uint64_t bd = tc::smem_desc_sw128(sb + PB[j] * C::HALVES * TILE_BYTES + ks * 32);
+                            const uint64_t bd = tc::smem_desc_sw128(sb + PB[j] * C::B_ROWS_BYTES + ks * 32);
                             tc::mma_bf16(dst, ad, bd, IDESC, accum);
                             accum = 1;
                         }
@@ -352,11 +403,11 @@ tc_gemm_kernel(const TcTask *__restrict__ tasks, const TcItem *__restrict__ item
         const int quarter = warp & 3, half = warp >> 2;
         const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
         uint32_t g = 0;
-        for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
-            const TcTask t = tasks[u / ncol];
-            const int col = u % ncol;
+        for (int u = blockIdx.x; u < la.nunits; u += gridDim.x) {
+            const TcUnit un = la.units[u];
+            const TcTask t = la.tasks[un.task];
             int ktiles = 0;
-            for (int q = 0; q < t.nitem; ++q) ktiles += items[t.item0 + q].KT;
+            for (int q = 0; q < t.nitem; ++q) ktiles += la.items[t.item0 + q].KT;
             float acc[C::COLS];
 #pragma unroll
             for (int e = 0; e < C::COLS; ++e) acc[e] = 0.f;
@@ -364,7 +415,7 @@ tc_gemm_kernel(const TcTask *__restrict__ tasks, const TcItem *__restrict__ item
             for (int i = 0; i < ktiles && ok; ++i, ++g) {
                 const int b = g & 1;
                 const uint32_t use = g >> 1;
-                if (!tc::mbar_wait(&accf[b], use & 1, abort_word, args.wait_cycles)) {
+                if (!tc::mbar_wait(&accf[b], use & 1, abort_word, la.wait_cycles)) {
                     *abort_word = 1;
                     ok = false;
                     break;
@@ -383,36 +434,38 @@ tc_gemm_kernel(const TcTask *__restrict__ tasks, const TcItem *__restrict__ item
                     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(tc::smem_u32(&acce[b])) : "memory");
             }
             if (!ok || *abort_word) break;
+            const PlanArgs *pa = la.plans + t.plan;
+            const int nrhs = pa->nrhs;
             const int r = t.m0 + quarter * 32 + lane;
-            const int beta = t.beta == 2 ? args.beta_arg : t.beta;
-            const int col0 = col * BN + half * C::COLS;
+            const int beta = t.beta == 2 ? pa->beta_arg : t.beta;
+            const int col0 = un.col * BN + half * C::COLS;
             // accumulating outputs: all old values of a 16-column chunk are loaded before any
             // store, so the loads overlap instead of waiting on each other
             if (t.out_kind == OUT_Y) {
                 if (r < t.M) {
-                    double *Yb = args.Y + args.yofs[t.c_row] + r;
+                    double *Yb = pa->Y + pa->yofs[t.c_row] + r;
 #pragma unroll
                     for (int c0 = 0; c0 < C::COLS; c0 += 16) {
                         double old[16];
 #pragma unroll
                         for (int e = 0; e < 16; ++e) {
                             const int cc = col0 + c0 + e;
-                            old[e] = (beta && cc < args.nrhs) ? Yb[(size_t)cc * t.ldc] : 0.0;
+                            old[e] = (beta && cc < nrhs) ? Yb[(size_t)cc * t.ldc] : 0.0;
                         }
 #pragma unroll
                         for (int e = 0; e < 16; ++e) {
                             const int cc = col0 + c0 + e;
-                            if (cc < args.nrhs) Yb[(size_t)cc * t.ldc] = old[e] + (double)acc[c0 + e];
+                            if (cc < nrhs) Yb[(size_t)cc * t.ldc] = old[e] + (double)acc[c0 + e];
                         }
                     }
                 }
             } else if (t.out_kind == OUT_F32) {
                 if (r < t.M) {
-                    float *Sb = args.skel + t.c_row * (int64_t)args.nrhs + r;
+                    float *Sb = pa->skel + t.c_row * (int64_t)nrhs + r;
 #pragma unroll
                     for (int e = 0; e < C::COLS; ++e) {
                         const int cc = col0 + e;
-                        if (cc < args.nrhs) Sb[(size_t)cc * t.ldc] = acc[e];
+                        if (cc < nrhs) Sb[(size_t)cc * t.ldc] = acc[e];
                     }
                 }
             } else {
@@ -422,14 +475,14 @@ tc_gemm_kernel(const TcTask *__restrict__ tasks, const TcItem *__restrict__ item
                 // per part.  Rows past M carry zeros (A is zero-padded); rows past the node's
                 // K tiles are not written.
                 if (beta && r < t.M) {
-                    const float *Sb = args.skel + t.c_row * (int64_t)args.nrhs + r;
+                    const float *Sb = pa->skel + t.c_row * (int64_t)nrhs + r;
 #pragma unroll
                     for (int c0 = 0; c0 < C::COLS; c0 += 16) {
                         float old[16];
 #pragma unroll
                         for (int e = 0; e < 16; ++e) {
                             const int cc = col0 + c0 + e;
-                            old[e] = cc < args.nrhs ? Sb[(size_t)cc * t.ldc] : 0.f;
+                            old[e] = cc < nrhs ? Sb[(size_t)cc * t.ldc] : 0.f;
                         }
 #pragma unroll
                         for (int e = 0; e < 16; ++e) acc[c0 + e] += old[e];
@@ -440,6 +493,8 @@ tc_gemm_kernel(const TcTask *__restrict__ tasks, const TcItem *__restrict__ item
                 const bool k_ok = k0 < KTv * 64;
                 const int kt = k0 >> 6;
                 const uint32_t kin = (uint32_t)(k0 & 63);
+                uint8_t *tbuf = pa->buf[la.t_buf];
+                const int NT = pa->NT;
 #pragma unroll
                 for (int g8 = 0; g8 < C::COLS / 8; ++g8) {
                     float x[8];
@@ -451,8 +506,8 @@ tc_gemm_kernel(const TcTask *__restrict__ tasks, const TcItem *__restrict__ item
 #pragma unroll
                     for (int j = 0; j < 8; ++j) tc::split3(x[j], h[j], m[j], l[j]);
                     if (k_ok) {
-                        uint8_t *tile0 = args.t_pool +
-                                         ((size_t)t.out_kt * args.NT + (size_t)(n >> 7) * KTv + kt) * 3 * (size_t)TILE_BYTES;
+                        uint8_t *tile0 = tbuf + ((size_t)t.out_kt * NT + (size_t)(n >> 7) * KTv + kt) * 3 *
+                                                    (size_t)TILE_BYTES;
                         store_parts(tile0, 3, n & 127, (int)(kin >> 3), h, m, l);
                     }
                 }
@@ -464,10 +519,10 @@ tc_gemm_kernel(const TcTask *__restrict__ tasks, const TcItem *__restrict__ item
     // all MMAs must be complete before TMEM is released (bounded, also after an abort)
     if (threadIdx.x == 0) {
         volatile int never = 0;
-        if (!tc::mbar_wait(doneb, 0, &never, args.wait_cycles)) *abort_word = 1;
+        if (!tc::mbar_wait(doneb, 0, &never, la.wait_cycles)) *abort_word = 1;
     }
     __syncthreads();
-    if (*abort_word && threadIdx.x == 0) atomicExch(args.err, MXB_ERR_TIMEOUT);
+    if (*abort_word && threadIdx.x == 0) atomicExch(la.err, MXB_ERR_TIMEOUT);
     tc::fence_before_sync();
     __syncthreads();
     if (warp == 0) tc::tmem_dealloc(tmem, C::TMEM_COLS);
@@ -475,51 +530,99 @@ tc_gemm_kernel(const TcTask *__restrict__ tasks, const TcItem *__restrict__ item
 
 int g_sm_count[128];
 
-template <int P, int BN>
-cudaError_t launch_tc(const TcTask *tasks, const TcItem *items, int ntasks, const TcArgs &a, cudaStream_t s)
+int sm_count()
 {
-    if (ntasks <= 0) return cudaSuccess;
-    using C = TcCfg<P, BN>;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return 148;
+    if (!g_sm_count[dev] && cudaDeviceGetAttribute(&g_sm_count[dev], cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return 148;
+    return g_sm_count[dev];
+}
+
+template <int P, int BN, int S>
+cudaError_t configure_tc()
+{
+    static bool done[128];
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 128) return cudaErrorInvalidDevice;
-    if (!g_sm_count[dev]) {
-        e = cudaDeviceGetAttribute(&g_sm_count[dev], cudaDevAttrMultiProcessorCount, dev);
-        if (e != cudaSuccess) return e;
-    }
-    static bool configured[128];
-    if (!configured[dev]) {
-        e = cudaFuncSetAttribute(tc_gemm_kernel<P, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
-        if (e != cudaSuccess) return e;
-        configured[dev] = true;
-    }
-    const int nunits = ntasks * ((a.nrhs + BN - 1) / BN);
-    const int grid = std::min(nunits, g_sm_count[dev]);
-    tc_gemm_kernel<P, BN><<<grid, C::THREADS, C::SMEM, s>>>(tasks, items, nunits, a);
+    if (done[dev]) return cudaSuccess;
+    e = cudaFuncSetAttribute(tc_gemm_kernel<P, BN, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             TcCfg<P, BN, S>::SMEM);
+    if (e == cudaSuccess) done[dev] = true;
+    return e;
+}
+
+template <int P, int BN, int S>
+cudaError_t launch_tc_cfg(const LaunchArgs &a, cudaStream_t s)
+{
+    if (a.nunits <= 0) return cudaSuccess;
+    cudaError_t e = configure_tc<P, BN, S>();
+    if (e != cudaSuccess) return e;
+    const int grid = std::min(a.nunits, sm_count());
+    tc_gemm_kernel<P, BN, S><<<grid, TcCfg<P, BN, S>::THREADS, TcCfg<P, BN, S>::SMEM, s>>>(a);
     return cudaGetLastError();
 }
 
-enum OpKind { OP_SPLIT_W, OP_SPLIT_WSKEL, OP_SPLIT_USKEL, OP_TC2, OP_TC3 };
-enum APool { POOL_NEAR, POOL_FAR, POOL_VU3, POOL_VD3, NPOOL };
-enum BBuf { BUF_W, BUF_WSKEL, BUF_USKEL };
+// Column-tile widths per product count; pipeline depth fills ~192-216 KiB of shared memory.
+cudaError_t launch_tc(int P, int BN, const LaunchArgs &a, cudaStream_t s)
+{
+    if (P == 2) {
+        if (BN == 256) return launch_tc_cfg<2, 256, 2>(a, s);
+        if (BN == 128) return launch_tc_cfg<2, 128, 3>(a, s);
+        return launch_tc_cfg<2, 64, 4>(a, s);
+    }
+    if (BN == 128) return launch_tc_cfg<3, 128, 2>(a, s);
+    return launch_tc_cfg<3, 64, 3>(a, s);
+}
 
-struct Op {
-    int kind, first, count, max_kt;
-    int a_pool, b_buf, t_buf;  // A pool, B buffer, tile buffer written by OUT_TILES tasks
-};
+cudaError_t configure_all_tc()
+{
+    cudaError_t e = configure_tc<2, 256, 2>();
+    if (e == cudaSuccess) e = configure_tc<2, 128, 3>();
+    if (e == cudaSuccess) e = configure_tc<2, 64, 4>();
+    if (e == cudaSuccess) e = configure_tc<3, 128, 2>();
+    if (e == cudaSuccess) e = configure_tc<3, 64, 3>();
+    return e;
+}
 
 int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// Position of an op in the evaluation sequence; ops of different plans with the same key run
+// in one launch.  W split, up-sweep by height, then for every depth far followed by down,
+// then near, then leaf down.
+enum OpPhase { PH_SPLITW = 0, PH_UP = 1, PH_FAR = 2, PH_DOWN = 3, PH_NEAR = 4, PH_LEAFDOWN = 5 };
+int64_t op_key(int phase, int level)
+{
+    switch (phase) {
+    case PH_SPLITW: return 0;
+    case PH_UP: return 1 + level;
+    case PH_FAR: return 100000 + 2 * (int64_t)level;
+    case PH_DOWN: return 100000 + 2 * (int64_t)level + 1;
+    case PH_NEAR: return 10000000;
+    default: return 10000001;
+    }
+}
+
+struct Op {             // one op of one plan
+    int64_t key;
+    int phase, P;
+    int a_pool, b_buf, t_buf;
+    int first, count;   // range in the plan's tasks (TC) or jobs (W split)
+};
+
+int batch_fail(const std::string &m, int code = MXB_ERR_ARG)
+{
+    set_error(m);
+    return code;
+}
 
 }  // namespace
 
 struct SplitBF16 {
     uint8_t *pool[NPOOL] = {};
     size_t pool_bytes[NPOOL] = {};
-    TcTask *dTasks = nullptr;
-    TcItem *dItems = nullptr;
-    SplitJob *dJobs = nullptr;
-    int *dErr = nullptr;
     std::vector<Op> ops;
     std::vector<TcTask> tasks;
     std::vector<TcItem> items;
@@ -529,7 +632,446 @@ struct SplitBF16 {
     int nt_cap = 0, nrhs_cap = 0;
     uint8_t *Wt = nullptr, *wT = nullptr, *uT = nullptr;
     float *u32 = nullptr;  // FP32 far results awaiting the down launch
+    int *dErr = nullptr;
+    Batch *self = nullptr;  // the single-plan batch used by mxb_plan_evaluate
 };
+
+// ---------------------------------------------------------------------------------------
+// batch: merged launch sequence of several split-BF16 plans
+// ---------------------------------------------------------------------------------------
+
+struct Batch : public mxb_batch {
+    std::vector<Plan *> plans;
+    struct MOp {
+        int64_t key;
+        int phase, P, a_pool, b_buf, t_buf;
+        int first, count;  // range in the merged tasks or jobs
+        int max_kt;
+    };
+    std::vector<MOp> ops;
+    std::vector<TcTask> tasks;
+    std::vector<TcItem> items;
+    std::vector<SplitJob> jobs;
+    TcTask *dTasks = nullptr;
+    TcItem *dItems = nullptr;
+    SplitJob *dJobs = nullptr;
+    std::vector<void *> allocations;
+    struct Entry {                     // one captured evaluation
+        std::vector<const double *> W;
+        std::vector<double *> Y;
+        std::vector<int> nrhs;
+        int accumulate = 0;
+        int debug_flags = 0;
+        std::vector<int> bn;           // column-tile width per op (0 for the W split)
+        PlanArgs *dPlans = nullptr;
+        TcUnit *dUnits = nullptr;
+        std::vector<int> unit_first, unit_count;
+        cudaGraphExec_t exec = nullptr;
+    };
+    std::vector<Entry> entries;
+    std::map<std::vector<int>, std::vector<int>> tuned;  // nrhs signature -> bn per op
+    cudaStream_t capture_stream = nullptr;
+    int device = 0;
+
+    ~Batch() override
+    {
+        clear();
+        if (capture_stream) cudaStreamDestroy(capture_stream);
+        for (void *p : allocations) cudaFree(p);
+    }
+    static void release(Entry &e)
+    {
+        if (e.exec) cudaGraphExecDestroy(e.exec);
+        if (e.dPlans) cudaFree(e.dPlans);
+        if (e.dUnits) cudaFree(e.dUnits);
+        e.exec = nullptr;
+        e.dPlans = nullptr;
+        e.dUnits = nullptr;
+    }
+    void clear()
+    {
+        for (Entry &e : entries) release(e);
+        entries.clear();
+    }
+    int build(const std::vector<Plan *> &ps);
+    int evaluate(const double *const *W, double *const *Y, const int *nrhs, int accumulate, cudaStream_t stream,
+                 int debug_flags, long long wait_cycles);
+    int enqueue(Entry &e, cudaStream_t stream, int debug_flags, long long wait_cycles, const std::vector<int> &bn,
+                int only_op = -1);
+    int units_for(Entry &e, const std::vector<int> &bn);
+    int tune(Entry &e, std::vector<PlanArgs> pa, std::vector<int> &bn, cudaStream_t stream, long long wait_cycles);
+};
+
+int Batch::build(const std::vector<Plan *> &ps)
+{
+    if (ps.empty()) return batch_fail("empty batch");
+    plans = ps;
+    const int prec = ps[0] ? ps[0]->precision : -1;
+    MXB_CUDA_OR(cudaGetDevice(&device));
+    for (Plan *p : ps) {
+        if (!p || !p->bf16) return batch_fail("batches take split-BF16 plans");
+        if (p->precision != prec) return batch_fail("all plans of a batch must use the same precision mode");
+        if (p->device != device) return batch_fail("all plans of a batch must live on the current device");
+    }
+    // merge ops by key, in key order; tasks and jobs get their plan index and offsets
+    std::map<int64_t, std::vector<std::pair<int, const Op *>>> by_key;
+    for (int pi = 0; pi < (int)ps.size(); ++pi)
+        for (const Op &o : ps[pi]->bf16->ops) by_key[o.key].push_back({pi, &o});
+    for (auto &kv : by_key) {
+        MOp m{};
+        m.key = kv.first;
+        const Op *o0 = kv.second[0].second;
+        m.phase = o0->phase;
+        m.P = o0->P;
+        m.a_pool = o0->a_pool;
+        m.b_buf = o0->b_buf;
+        m.t_buf = o0->t_buf;
+        m.max_kt = 1;
+        if (m.phase == PH_SPLITW) {
+            m.first = (int)jobs.size();
+            for (auto &po : kv.second) {
+                const SplitBF16 &S = *ps[po.first]->bf16;
+                for (int j = po.second->first; j < po.second->first + po.second->count; ++j) {
+                    SplitJob sj = S.jobs[j];
+                    sj.plan = po.first;
+                    m.max_kt = std::max(m.max_kt, sj.KT);
+                    jobs.push_back(sj);
+                }
+            }
+            m.count = (int)jobs.size() - m.first;
+        } else {
+            m.first = (int)tasks.size();
+            for (auto &po : kv.second) {
+                const SplitBF16 &S = *ps[po.first]->bf16;
+                if (po.second->P != m.P) return batch_fail("plans disagree on a launch's product count");
+                for (int j = po.second->first; j < po.second->first + po.second->count; ++j) {
+                    TcTask t = S.tasks[j];
+                    const int item0 = (int)items.size();
+                    for (int q = 0; q < t.nitem; ++q) items.push_back(S.items[t.item0 + q]);
+                    t.item0 = item0;
+                    t.plan = po.first;
+                    tasks.push_back(t);
+                }
+            }
+            m.count = (int)tasks.size() - m.first;
+            // longest tasks first: balances the persistent kernel's static round-robin
+            auto cost = [&](const TcTask &t) {
+                int k = 0;
+                for (int q = 0; q < t.nitem; ++q) k += items[t.item0 + q].KT;
+                return k;
+            };
+            std::stable_sort(tasks.begin() + m.first, tasks.end(),
+                             [&](const TcTask &a, const TcTask &b) { return cost(a) > cost(b); });
+        }
+        if (m.count > 0) ops.push_back(m);
+    }
+    auto up = [&](void **dst, const void *src, size_t bytes) -> int {
+        cudaError_t e = cudaMalloc(dst, std::max<size_t>(bytes, 16));
+        if (e != cudaSuccess) return batch_fail(std::string("batch allocation: ") + cudaGetErrorString(e), MXB_ERR_NOMEM);
+        allocations.push_back(*dst);
+        if (bytes) e = cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return batch_fail(std::string("batch upload: ") + cudaGetErrorString(e), MXB_ERR_CUDA);
+        return MXB_OK;
+    };
+    int rc = up((void **)&dTasks, tasks.data(), tasks.size() * sizeof(TcTask));
+    if (!rc) rc = up((void **)&dItems, items.data(), items.size() * sizeof(TcItem));
+    if (!rc) rc = up((void **)&dJobs, jobs.data(), jobs.size() * sizeof(SplitJob));
+    return rc;
+}
+
+// Work units of every TC op for this entry's nrhs and column-tile choices.
+int Batch::units_for(Entry &e, const std::vector<int> &bn)
+{
+    std::vector<TcUnit> units;
+    e.unit_first.assign(ops.size(), 0);
+    e.unit_count.assign(ops.size(), 0);
+    for (size_t k = 0; k < ops.size(); ++k) {
+        const MOp &m = ops[k];
+        e.unit_first[k] = (int)units.size();
+        if (m.phase == PH_SPLITW) continue;
+        for (int t = m.first; t < m.first + m.count; ++t) {
+            const int ncol = (int)ceil_div(e.nrhs[tasks[t].plan], bn[k]);
+            for (int c = 0; c < ncol; ++c) units.push_back(TcUnit{t, c});
+        }
+        e.unit_count[k] = (int)units.size() - e.unit_first[k];
+    }
+    if (e.dUnits) cudaFree(e.dUnits);
+    e.dUnits = nullptr;
+    cudaError_t err = cudaMalloc(&e.dUnits, std::max<size_t>(units.size(), 1) * sizeof(TcUnit));
+    if (err == cudaSuccess && !units.empty())
+        err = cudaMemcpy(e.dUnits, units.data(), units.size() * sizeof(TcUnit), cudaMemcpyHostToDevice);
+    if (err != cudaSuccess) return batch_fail(std::string("work units: ") + cudaGetErrorString(err), MXB_ERR_CUDA);
+    return MXB_OK;
+}
+
+int Batch::enqueue(Entry &e, cudaStream_t stream, int debug_flags, long long wait_cycles, const std::vector<int> &bn,
+                   int only_op)
+{
+    bool first_tc = true;
+    int maxnt = 0;
+    for (Plan *p : plans) maxnt = std::max(maxnt, p->bf16->nt_cap);
+    for (size_t k = 0; k < ops.size(); ++k) {
+        const MOp &m = ops[k];
+        const bool run = only_op < 0 || (int)k == only_op;
+        cudaError_t err = cudaSuccess;
+        if (m.phase == PH_SPLITW) {
+            if (run) {
+                split_w_kernel<<<dim3(m.count, m.max_kt, maxnt), 256, 0, stream>>>(dJobs + m.first, e.dPlans);
+                err = cudaGetLastError();
+            }
+        } else {
+            if (run) {
+                LaunchArgs a{};
+                a.plans = e.dPlans;
+                a.tasks = dTasks;
+                a.items = dItems;
+                a.units = e.dUnits + e.unit_first[k];
+                a.nunits = e.unit_count[k];
+                a.a_pool = m.a_pool;
+                a.b_buf = m.b_buf;
+                a.t_buf = m.t_buf < 0 ? 0 : m.t_buf;
+                a.err = plans[0]->bf16->dErr;
+                a.wait_cycles = wait_cycles > 0 ? wait_cycles : tc::WAIT_CYCLES;
+                a.stall_test = (debug_flags & MXB_DEBUG_STALL_ONE_WAIT) && first_tc;
+                err = launch_tc(m.P, bn[k], a, stream);
+            }
+            first_tc = false;
+        }
+        if (err != cudaSuccess) return batch_fail(std::string("split-BF16 launch: ") + cudaGetErrorString(err), MXB_ERR_CUDA);
+    }
+    return MXB_OK;
+}
+
+namespace {
+
+int split_buffers(Plan &p, SplitBF16 &S, int nrhs)
+{
+    const int NT = 2 * (int)ceil_div(nrhs, 256);  // even: BN = 256 launches read tile pairs
+    if (NT <= S.nt_cap && nrhs <= S.nrhs_cap) return MXB_OK;
+    auto release = [&](void *q) {
+        if (!q) return;
+        cudaFree(q);
+        p.allocations.erase(std::remove(p.allocations.begin(), p.allocations.end(), q), p.allocations.end());
+    };
+    release(S.Wt);
+    release(S.wT);
+    release(S.uT);
+    release(S.u32);
+    S.Wt = S.wT = S.uT = nullptr;
+    S.u32 = nullptr;
+    const size_t tile3 = 3 * (size_t)TILE_BYTES;
+    int rc = p.alloc((void **)&S.Wt, std::max<int64_t>(S.leaf_kt_total, 1) * NT * tile3);
+    if (!rc) rc = p.alloc((void **)&S.wT, std::max<int64_t>(S.node_kt_total, 1) * NT * tile3);
+    if (!rc) rc = p.alloc((void **)&S.uT, std::max<int64_t>(S.node_kt_total, 1) * NT * tile3);
+    if (!rc) rc = p.alloc((void **)&S.u32, std::max<int64_t>(p.skel_total, 1) * (size_t)nrhs * sizeof(float));
+    if (rc) return rc;
+    S.nt_cap = NT;
+    S.nrhs_cap = nrhs;
+    return MXB_OK;
+}
+
+// Default column tile: the widest that the right-hand sides fill.
+int default_bn(int P, int nrhs_max)
+{
+    if (P == 2) return nrhs_max > 128 ? 256 : (nrhs_max > 64 ? 128 : 64);
+    return nrhs_max > 64 ? 128 : 64;
+}
+
+bool autotune_enabled()
+{
+    static const bool on = [] {
+        const char *e = getenv("MXB_AUTOTUNE");
+        return !(e && *e == '0');
+    }();
+    return on;
+}
+
+}  // namespace
+
+// Autotuner: runs the op sequence once; every tensor-core op is timed with each candidate
+// column-tile width (second of two runs, CUDA events) with the Y outputs redirected to
+// scratch, and the fastest width is kept.  Each op's outputs are left in place for the next.
+int Batch::tune(Entry &e, std::vector<PlanArgs> pa, std::vector<int> &bn, cudaStream_t stream, long long wait_cycles)
+{
+    const int np = (int)plans.size();
+    const int maxn = *std::max_element(e.nrhs.begin(), e.nrhs.end());
+    std::vector<double *> scratch(np, nullptr);
+    PlanArgs *dTune = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    Entry te;
+    te.nrhs = e.nrhs;
+    int rc = MXB_OK;
+    for (int i = 0; i < np && !rc; ++i) {
+        Plan &p = *plans[i];
+        size_t ext = 0;
+        for (int l = 0; l < p.nleaf; ++l)
+            ext = std::max<size_t>(ext, (size_t)p.ofs_host[1][l] + (size_t)p.Ddim[l] * e.nrhs[i]);
+        if (cudaMalloc(&scratch[i], std::max<size_t>(ext, 1) * sizeof(double)) != cudaSuccess)
+            rc = batch_fail("autotune scratch allocation failed", MXB_ERR_NOMEM);
+        else
+            pa[i].Y = scratch[i];
+    }
+    if (!rc && cudaMalloc(&dTune, np * sizeof(PlanArgs)) != cudaSuccess)
+        rc = batch_fail("autotune table allocation failed", MXB_ERR_NOMEM);
+    if (!rc && cudaMemcpy(dTune, pa.data(), np * sizeof(PlanArgs), cudaMemcpyHostToDevice) != cudaSuccess)
+        rc = batch_fail("autotune table upload failed", MXB_ERR_CUDA);
+    te.dPlans = dTune;
+    if (!rc && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
+        rc = batch_fail("autotune events", MXB_ERR_CUDA);
+    for (size_t k = 0; k < ops.size() && !rc; ++k) {
+        if (ops[k].phase == PH_SPLITW) {
+            rc = units_for(te, bn);
+            if (!rc) rc = enqueue(te, stream, 0, wait_cycles, bn, (int)k);
+            continue;
+        }
+        const std::vector<int> cands = ops[k].P == 2 ? std::vector<int>{256, 128, 64} : std::vector<int>{128, 64};
+        float best = 1e30f;
+        int best_bn = bn[k];
+        for (int c : cands) {
+            if (c > 2 * std::max(64, maxn)) continue;
+            std::vector<int> trial = bn;
+            trial[k] = c;
+            rc = units_for(te, trial);
+            float ms = 0.f;
+            for (int rep = 0; rep < 2 && !rc; ++rep) {
+                cudaEventRecord(e0, stream);
+                rc = enqueue(te, stream, 0, wait_cycles, trial, (int)k);
+                cudaEventRecord(e1, stream);
+                if (!rc && cudaEventSynchronize(e1) != cudaSuccess) rc = batch_fail("autotune sync", MXB_ERR_CUDA);
+                if (!rc) cudaEventElapsedTime(&ms, e0, e1);
+            }
+            if (rc) break;
+            if (ms < best) {
+                best = ms;
+                best_bn = c;
+            }
+        }
+        bn[k] = best_bn;
+        if (!rc) rc = units_for(te, bn);
+        if (!rc) rc = enqueue(te, stream, 0, wait_cycles, bn, (int)k);
+    }
+    if (!rc && cudaStreamSynchronize(stream) != cudaSuccess) rc = batch_fail("autotune sync", MXB_ERR_CUDA);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (te.dUnits) cudaFree(te.dUnits);
+    if (dTune) cudaFree(dTune);
+    for (double *s : scratch)
+        if (s) cudaFree(s);
+    return rc;
+}
+
+int Batch::evaluate(const double *const *W, double *const *Y, const int *nrhs, int accumulate, cudaStream_t stream,
+                    int debug_flags, long long wait_cycles)
+{
+    const int np = (int)plans.size();
+    int cur = -1;
+    MXB_CUDA_OR(cudaGetDevice(&cur));
+    if (cur != device) return batch_fail("batch used on a different device than it was created on");
+    std::vector<int> nr(nrhs, nrhs + np);
+    bool realloc = false;
+    for (int i = 0; i < np; ++i) {
+        if (nr[i] < 1 || !W[i] || !Y[i]) return batch_fail("bad operand or nrhs in batch");
+        const int nt0 = plans[i]->bf16->nt_cap, nr0 = plans[i]->bf16->nrhs_cap;
+        int rc = split_buffers(*plans[i], *plans[i]->bf16, nr[i]);
+        if (rc) return rc;
+        realloc |= plans[i]->bf16->nt_cap != nt0 || plans[i]->bf16->nrhs_cap != nr0;
+    }
+    if (realloc) clear();
+    MXB_CUDA_OR(configure_all_tc());
+    Entry *hit = nullptr;
+    for (Entry &e : entries) {
+        bool same = e.accumulate == accumulate && e.nrhs == nr && e.debug_flags == debug_flags;
+        for (int i = 0; same && i < np; ++i) same = e.W[i] == W[i] && e.Y[i] == Y[i];
+        if (same) hit = &e;
+    }
+    if (!hit) {
+        if (entries.size() >= 8) {
+            release(entries.front());
+            entries.erase(entries.begin());
+        }
+        Entry e;
+        e.W.assign(W, W + np);
+        e.Y.assign(Y, Y + np);
+        e.nrhs = nr;
+        e.accumulate = accumulate;
+        e.debug_flags = debug_flags;
+        std::vector<PlanArgs> pa(np);
+        for (int i = 0; i < np; ++i) {
+            Plan &p = *plans[i];
+            SplitBF16 &S = *p.bf16;
+            for (int k = 0; k < NPOOL; ++k) pa[i].pool[k] = S.pool[k];
+            pa[i].buf[BUF_W] = S.Wt;
+            pa[i].buf[BUF_WSKEL] = S.wT;
+            pa[i].buf[BUF_USKEL] = S.uT;
+            pa[i].W = W[i];
+            pa[i].Y = Y[i];
+            pa[i].wofs = p.dOfs;
+            pa[i].yofs = p.dOfs + p.nleaf;
+            pa[i].skel = S.u32;
+            pa[i].NT = S.nt_cap;
+            pa[i].nrhs = nr[i];
+            pa[i].beta_arg = accumulate ? 1 : 0;
+        }
+        cudaError_t err = cudaMalloc(&e.dPlans, np * sizeof(PlanArgs));
+        if (err == cudaSuccess) err = cudaMemcpy(e.dPlans, pa.data(), np * sizeof(PlanArgs), cudaMemcpyHostToDevice);
+        if (err != cudaSuccess) {
+            release(e);
+            return batch_fail(std::string("batch plan table: ") + cudaGetErrorString(err), MXB_ERR_CUDA);
+        }
+        // column tiles: measured per op on the first evaluation of an nrhs signature
+        const int maxn = *std::max_element(nr.begin(), nr.end());
+        std::vector<int> bn(ops.size(), 0);
+        for (size_t k = 0; k < ops.size(); ++k)
+            if (ops[k].phase != PH_SPLITW) bn[k] = default_bn(ops[k].P, maxn);
+        auto t = tuned.find(nr);
+        if (t != tuned.end()) {
+            bn = t->second;
+        } else if (autotune_enabled() && !debug_flags) {
+            int rc = tune(e, pa, bn, stream, wait_cycles);
+            if (rc) {
+                release(e);
+                return rc;
+            }
+            tuned[nr] = bn;
+        }
+        e.bn = bn;
+        int rc = units_for(e, bn);
+        if (rc) {
+            release(e);
+            return rc;
+        }
+        if (!capture_stream && cudaStreamCreateWithFlags(&capture_stream, cudaStreamNonBlocking) != cudaSuccess) {
+            release(e);
+            return batch_fail("creating the capture stream failed", MXB_ERR_CUDA);
+        }
+        if (cudaStreamBeginCapture(capture_stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            release(e);
+            return batch_fail("beginning the graph capture failed", MXB_ERR_CUDA);
+        }
+        rc = enqueue(e, capture_stream, debug_flags, wait_cycles, bn);
+        cudaGraph_t graph = nullptr;
+        err = cudaStreamEndCapture(capture_stream, &graph);
+        if (rc || err != cudaSuccess) {
+            if (graph) cudaGraphDestroy(graph);
+            release(e);
+            return rc ? rc : batch_fail(std::string("capturing the evaluation: ") + cudaGetErrorString(err), MXB_ERR_CUDA);
+        }
+        err = cudaGraphInstantiate(&e.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (err != cudaSuccess) {
+            release(e);
+            return batch_fail(std::string("instantiating the evaluation graph: ") + cudaGetErrorString(err), MXB_ERR_CUDA);
+        }
+        entries.push_back(std::move(e));
+        hit = &entries.back();
+    }
+    MXB_CUDA_OR(cudaGraphLaunch(hit->exec, stream));
+    return MXB_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// plan set-up
+// ---------------------------------------------------------------------------------------
 
 int Plan::setup_split_bf16(const mxb_cds_desc &)
 {
@@ -628,31 +1170,20 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
         maxh = std::max(maxh, height[v]);
         maxd = std::max(maxd, depth[v]);
     }
-    auto begin_op = [&](int kind, int a_pool, int b_buf, int t_buf) {
+    auto begin_op = [&](int phase, int level, int P, int a_pool, int b_buf, int t_buf) {
         Op o{};
-        o.kind = kind;
+        o.key = op_key(phase, level);
+        o.phase = phase;
+        o.P = P;
         o.a_pool = a_pool;
         o.b_buf = b_buf;
         o.t_buf = t_buf;
-        o.first = (kind <= OP_SPLIT_USKEL) ? (int)S->jobs.size() : (int)S->tasks.size();
+        o.first = phase == PH_SPLITW ? (int)S->jobs.size() : (int)S->tasks.size();
         S->ops.push_back(o);
     };
     auto end_op = [&]() {
         Op &o = S->ops.back();
-        if (o.kind >= OP_TC2) {
-            // longest tasks first: balances the persistent kernel's static round-robin
-            auto cost = [&](const TcTask &t) {
-                int k = 0;
-                for (int q = 0; q < t.nitem; ++q) k += S->items[t.item0 + q].KT;
-                return k;
-            };
-            std::stable_sort(S->tasks.begin() + o.first, S->tasks.end(),
-                             [&](const TcTask &a, const TcTask &b) { return cost(a) > cost(b); });
-        }
-        o.count = ((o.kind <= OP_SPLIT_USKEL) ? (int)S->jobs.size() : (int)S->tasks.size()) - o.first;
-        o.max_kt = 1;
-        if (o.kind <= OP_SPLIT_USKEL)
-            for (int j = o.first; j < o.first + o.count; ++j) o.max_kt = std::max(o.max_kt, S->jobs[j].KT);
+        o.count = (o.phase == PH_SPLITW ? (int)S->jobs.size() : (int)S->tasks.size()) - o.first;
         if (o.count == 0) S->ops.pop_back();
     };
     auto add_tasks = [&](int16_t out_kind, int64_t c_row, int64_t out_kt, int ldc, int M, int item0,
@@ -666,6 +1197,7 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
             t.m0 = m0;
             t.item0 = item0;
             t.nitem = (int)S->items.size() - item0;
+            t.plan = 0;
             t.out_kind = out_kind;
             t.beta = beta;
             S->tasks.push_back(t);
@@ -678,23 +1210,23 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
         it.KT = KT(K);
         if (it.KT > 0) S->items.push_back(it);
     };
-    auto split_job = [&](int64_t src_row, int64_t dst_kt, int ld, int K) {
-        SplitJob j{};
-        j.src_row = src_row;
-        j.dst_kt = dst_kt;
-        j.ld = ld;
-        j.K = K;
-        j.KT = KT(K);
-        if (j.KT > 0) S->jobs.push_back(j);
-    };
 
     // W -> tiles
-    begin_op(OP_SPLIT_W, -1, BUF_W, -1);
-    for (int i = 0; i < nleaf; ++i) split_job(i, S->leaf_kt[i], Ddim[i], Ddim[i]);
+    begin_op(PH_SPLITW, 0, 0, -1, BUF_W, -1);
+    for (int i = 0; i < nleaf; ++i) {
+        SplitJob j{};
+        j.src_row = i;
+        j.dst_kt = S->leaf_kt[i];
+        j.ld = Ddim[i];
+        j.K = Ddim[i];
+        j.KT = KT(Ddim[i]);
+        j.plan = 0;
+        if (j.KT > 0) S->jobs.push_back(j);
+    }
     end_op();
     // up-sweep by height: the epilogue writes wskel directly as operand tiles
     for (int h = 0; h <= maxh; ++h) {
-        begin_op(OP_TC3, POOL_VU3, h == 0 ? BUF_W : BUF_WSKEL, BUF_WSKEL);
+        begin_op(PH_UP, h, 3, POOL_VU3, h == 0 ? BUF_W : BUF_WSKEL, BUF_WSKEL);
         for (int v : bfs) {
             if (height[v] != h || !projects(v)) continue;
             const int item0 = (int)S->items.size();
@@ -715,7 +1247,7 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
     std::vector<std::vector<int>> far_out(numnodes);
     for (size_t k = 0; k < far_x.size(); ++k) far_out[far_x[k]].push_back((int)k);
     for (int dd = 1; dd <= maxd; ++dd) {
-        begin_op(far_parts == 2 ? OP_TC2 : OP_TC3, POOL_FAR, BUF_WSKEL, BUF_USKEL);
+        begin_op(PH_FAR, dd, far_parts, POOL_FAR, BUF_WSKEL, BUF_USKEL);
         for (int c : bfs) {
             if (depth[c] != dd || !projects(c)) continue;
             const int item0 = (int)S->items.size();
@@ -724,7 +1256,7 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
             add_tasks(has_down(c) ? OUT_F32 : OUT_TILES, skel_row[c], S->node_kt[c], slen[c], slen[c], item0, 0);
         }
         end_op();
-        begin_op(OP_TC3, POOL_VD3, BUF_USKEL, BUF_USKEL);
+        begin_op(PH_DOWN, dd, 3, POOL_VD3, BUF_USKEL, BUF_USKEL);
         for (int c : bfs) {
             if (depth[c] != dd || !projects(c) || !has_down(c)) continue;
             const int item0 = (int)S->items.size();
@@ -736,7 +1268,7 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
     // near (Y (+)= D W) then leaf down (Y += P^T uskel)
     std::vector<std::vector<int>> near_out(nleaf);
     for (size_t k = 0; k < near_x.size(); ++k) near_out[near_x[k]].push_back((int)k);
-    begin_op(near_parts == 2 ? OP_TC2 : OP_TC3, POOL_NEAR, BUF_W, -1);
+    begin_op(PH_NEAR, 0, near_parts, POOL_NEAR, BUF_W, -1);
     for (int v : bfs) {
         if (lch[v] != -1) continue;
         const int x = lm[v];
@@ -745,7 +1277,7 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
         add_tasks(OUT_Y, x, 0, Ddim[x], Ddim[x], item0, 2);
     }
     end_op();
-    begin_op(OP_TC3, POOL_VD3, BUF_USKEL, -1);
+    begin_op(PH_LEAFDOWN, 0, 3, POOL_VD3, BUF_USKEL, -1);
     for (int v : bfs) {
         if (lch[v] != -1 || !projects(v)) continue;
         const int item0 = (int)S->items.size();
@@ -754,57 +1286,15 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
     }
     end_op();
 
-    int rc = alloc((void **)&S->dTasks, std::max<size_t>(S->tasks.size(), 1) * sizeof(TcTask));
-    if (!rc) rc = alloc((void **)&S->dItems, std::max<size_t>(S->items.size(), 1) * sizeof(TcItem));
-    if (!rc) rc = alloc((void **)&S->dJobs, std::max<size_t>(S->jobs.size(), 1) * sizeof(SplitJob));
-    if (!rc) rc = alloc((void **)&S->dErr, sizeof(int));
+    int rc = alloc((void **)&S->dErr, sizeof(int));
     if (rc) return rc;
-    cudaError_t e = cudaMemcpy(S->dTasks, S->tasks.data(), S->tasks.size() * sizeof(TcTask), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess && !S->items.empty())
-        e = cudaMemcpy(S->dItems, S->items.data(), S->items.size() * sizeof(TcItem), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess && !S->jobs.empty())
-        e = cudaMemcpy(S->dJobs, S->jobs.data(), S->jobs.size() * sizeof(SplitJob), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemset(S->dErr, 0, sizeof(int));
-    if (e != cudaSuccess) {
-        set_error(std::string("uploading split-BF16 task lists: ") + cudaGetErrorString(e));
+    if (cudaMemset(S->dErr, 0, sizeof(int)) != cudaSuccess) {
+        set_error("clearing the error word failed");
         return MXB_ERR_CUDA;
     }
-    return MXB_OK;
-}
-
-static int split_buffers(Plan &p, SplitBF16 &S, int nrhs)
-{
-    const int NT = 2 * (int)ceil_div(nrhs, 256);  // even: BN = 256 launches read tile pairs
-    if (NT <= S.nt_cap && nrhs <= S.nrhs_cap) return MXB_OK;
-    auto release = [&](void *q) {
-        if (!q) return;
-        cudaFree(q);
-        p.allocations.erase(std::remove(p.allocations.begin(), p.allocations.end(), q), p.allocations.end());
-    };
-    release(S.Wt);
-    release(S.wT);
-    release(S.uT);
-    release(S.u32);
-    S.Wt = S.wT = S.uT = nullptr;
-    S.u32 = nullptr;
-    const size_t tile3 = 3 * (size_t)TILE_BYTES;
-    int rc = p.alloc((void **)&S.Wt, std::max<int64_t>(S.leaf_kt_total, 1) * NT * tile3);
-    if (!rc) rc = p.alloc((void **)&S.wT, std::max<int64_t>(S.node_kt_total, 1) * NT * tile3);
-    if (!rc) rc = p.alloc((void **)&S.uT, std::max<int64_t>(S.node_kt_total, 1) * NT * tile3);
-    if (!rc) rc = p.alloc((void **)&S.u32, std::max<int64_t>(p.skel_total, 1) * (size_t)nrhs * sizeof(float));
-    if (rc) return rc;
-    S.nt_cap = NT;
-    S.nrhs_cap = nrhs;
-    return MXB_OK;
-}
-
-int Plan::prepare_split_bf16(int nrhs, bool *reallocated)
-{
-    const int nt_before = bf16->nt_cap, n_before = bf16->nrhs_cap;
-    int rc = split_buffers(*this, *bf16, nrhs);
-    if (rc) return rc;
-    *reallocated = bf16->nt_cap != nt_before || bf16->nrhs_cap != n_before;
-    return split_bf16_prepare();
+    // the batch of this plan alone, used by mxb_plan_evaluate
+    S->self = new Batch();
+    return S->self->build({this});
 }
 
 int Plan::run_split_bf16(const std::vector<Launch> &L, const double *dW, double *dY, int nrhs, int accumulate,
@@ -814,62 +1304,17 @@ int Plan::run_split_bf16(const std::vector<Launch> &L, const double *dW, double 
         set_error("the adjoint runs in FP64 mode only (create an FP64 plan for mxb_plan_adjoint)");
         return MXB_ERR_UNSUPPORTED;
     }
-    SplitBF16 &S = *bf16;
-    const int NT = S.nt_cap;
-    cudaError_t e = cudaSuccess;
-    bool first_tc = true;
-    for (const Op &o : S.ops) {
-        switch (o.kind) {
-        case OP_SPLIT_W:
-            split_b_kernel<double><<<dim3(o.count, o.max_kt, NT), 256, 0, stream>>>(S.dJobs + o.first, dW, dOfs,
-                                                                                  nrhs, NT, S.Wt);
-            break;
-        default: {
-            TcArgs a{};
-            a.a_pool = S.pool[o.a_pool];
-            a.b_pool = o.b_buf == BUF_W ? S.Wt : (o.b_buf == BUF_WSKEL ? S.wT : S.uT);
-            a.t_pool = o.t_buf == BUF_WSKEL ? S.wT : S.uT;
-            a.Y = dY;
-            a.yofs = dOfs + nleaf;
-            a.err = S.dErr;
-            a.NT = NT;
-            a.nrhs = nrhs;
-            a.skel = S.u32;
-            a.beta_arg = accumulate ? 1 : 0;
-            a.wait_cycles = debug_wait_cycles > 0 ? debug_wait_cycles : tc::WAIT_CYCLES;
-            a.stall_test = (debug_flags & MXB_DEBUG_STALL_ONE_WAIT) && first_tc;
-            first_tc = false;
-            if (o.kind == OP_TC2) e = launch_tc<2, 256>(S.dTasks + o.first, S.dItems, o.count, a, stream);
-            else e = launch_tc<3, 128>(S.dTasks + o.first, S.dItems, o.count, a, stream);
-            break;
-        }
-        }
-        if (e == cudaSuccess) e = cudaGetLastError();
-        if (e != cudaSuccess) {
-            set_error(std::string("split-BF16 launch: ") + cudaGetErrorString(e));
-            return MXB_ERR_CUDA;
-        }
-    }
-    return MXB_OK;
+    return bf16->self->evaluate(&dW, &dY, &nrhs, accumulate, stream, debug_flags, debug_wait_cycles);
 }
 
-int split_bf16_prepare()
+void Plan::clear_split_graphs()
 {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return MXB_ERR_CUDA;
-    if (!g_sm_count[dev] && cudaDeviceGetAttribute(&g_sm_count[dev], cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
-        return MXB_ERR_CUDA;
-    if (cudaFuncSetAttribute(tc_gemm_kernel<2, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             TcCfg<2, 256>::SMEM) != cudaSuccess ||
-        cudaFuncSetAttribute(tc_gemm_kernel<3, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             TcCfg<3, 128>::SMEM) != cudaSuccess) {
-        set_error("configuring the tensor-core kernels' shared memory failed");
-        return MXB_ERR_CUDA;
-    }
-    return MXB_OK;
+    if (bf16 && bf16->self) bf16->self->clear();
 }
 
-int split_bf16_launches(const Plan &p) { return p.bf16 ? (int)p.bf16->ops.size() : 0; }
+int split_bf16_prepare() { return configure_all_tc() == cudaSuccess ? MXB_OK : MXB_ERR_CUDA; }
+
+int split_bf16_launches(const Plan &p) { return p.bf16 ? (int)p.bf16->self->ops.size() : 0; }
 
 int split_bf16_status(Plan &p)
 {
@@ -890,8 +1335,59 @@ int split_bf16_status(Plan &p)
 
 void Plan::free_split_bf16()
 {
+    if (bf16) delete bf16->self;
     delete bf16;
     bf16 = nullptr;
+}
+
+// ---- batch entry points used by the C-ABI ----
+int batch_create(Plan *const *plans, int count, Batch **out)
+{
+    if (!plans || count < 1 || !out) return batch_fail("bad batch arguments");
+    std::unique_ptr<Batch> b(new Batch());
+    int rc = b->build(std::vector<Plan *>(plans, plans + count));
+    if (rc) return rc;
+    *out = b.release();
+    return MXB_OK;
+}
+
+int batch_evaluate(Batch *b, const double *const *W, double *const *Y, const int *nrhs, int accumulate,
+                   cudaStream_t stream)
+{
+    if (!b || !W || !Y || !nrhs) return batch_fail("bad batch arguments");
+    for (size_t i = 0; i < b->plans.size(); ++i) {
+        if (nrhs[i] < 1) return batch_fail("nrhs must be >= 1");
+        int rc = b->plans[i]->stage_offsets(0, nullptr, nrhs[i], stream);
+        if (!rc) rc = b->plans[i]->stage_offsets(1, nullptr, nrhs[i], stream);
+        if (rc) return rc;
+    }
+    return b->evaluate(W, Y, nrhs, accumulate, stream, 0, 0);
+}
+
+int batch_status(Batch *b)
+{
+    if (!b) return batch_fail("null batch");
+    MXB_CUDA_OR(cudaDeviceSynchronize());
+    int rc = MXB_OK;
+    for (Plan *p : b->plans) {
+        const int r = split_bf16_status(*p);
+        if (r && !rc) rc = r;
+    }
+    return rc;
+}
+
+void batch_destroy(Batch *b) { delete b; }
+
+int batch_launches(const Batch *b) { return b ? (int)b->ops.size() : 0; }
+
+int batch_tuned_widths(const Batch *b, int *widths, int cap)
+{
+    if (!b || b->entries.empty()) return 0;
+    const std::vector<int> &bn = b->entries.back().bn;
+    int n = 0;
+    for (size_t k = 0; k < bn.size() && n < cap; ++k)
+        if (bn[k]) widths[n++] = bn[k];
+    return n;
 }
 
 }  // namespace mxb

@@ -271,6 +271,60 @@ class Plan:
         return out
 
 
+class Batch:
+    """Several split-BF16 plans evaluated by one merged, graph-captured launch sequence
+    (``mxb_batch_*``); the column-tile widths are tuned by measurement on first use."""
+
+    def __init__(self, plans):
+        if not plans:
+            raise ValueError("empty batch")
+        self.plans = list(plans)  # the plans must outlive the batch
+        arr = (P * len(self.plans))(*[p._h for p in self.plans])
+        h = P()
+        check(_lib.load().mxb_batch_create(arr, len(self.plans), ctypes.byref(h)), "mxb_batch_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().mxb_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def evaluate(self, TWs, nrhs, outs=None, accumulate=False, stream=None):
+        """outs[i] (+)= K~_i TWs[i] for every plan i (packed leaf-blocked float64 CUDA tensors)."""
+        torch = _torch()
+        n = len(self.plans)
+        if len(TWs) != n or len(nrhs) != n:
+            raise ValueError("one operand and one nrhs per plan")
+        if outs is None:
+            outs = [torch.zeros(p.n * r, dtype=torch.float64, device=t.device)
+                    for p, r, t in zip(self.plans, nrhs, TWs)]
+            accumulate = False
+        for p, r, t, o in zip(self.plans, nrhs, TWs, outs):
+            p._check_operand(t, r)
+            p._check_operand(o, r)
+        W = (P * n)(*[t.data_ptr() for t in TWs])
+        Y = (P * n)(*[o.data_ptr() for o in outs])
+        R = (I32 * n)(*[int(r) for r in nrhs])
+        check(_lib.load().mxb_batch_evaluate(self._h, W, Y, R, int(accumulate), _stream_ptr(stream)),
+              "mxb_batch_evaluate")
+        return outs
+
+    def status(self) -> None:
+        check(_lib.load().mxb_batch_status(self._h), "mxb_batch_status")
+
+    def info(self):
+        l, nw = I32(), I32()
+        widths = (I32 * 256)()
+        check(_lib.load().mxb_batch_info(self._h, ctypes.byref(l), widths, 256, ctypes.byref(nw)), "mxb_batch_info")
+        return {"launches": int(l.value), "widths": [int(widths[i]) for i in range(nw.value)]}
+
+
 class Evaluator:
     """Y = K~ W with W, Y as (N, r) float64 CUDA tensors in the caller's point order."""
 
