@@ -481,7 +481,7 @@ int Plan::run(const std::vector<Launch> &L, const double *dW, double *dY, int nr
         set_error("plan used on a different device than it was created on");
         return MXB_ERR_ARG;
     }
-    int rc = ensure_scratch(nrhs);
+    int rc = precision == MXB_PREC_FP64 ? ensure_scratch(nrhs) : MXB_OK;  // FP64 skeleton scratch
     if (rc) return rc;
     rc = stage_offsets(0, wofs, nrhs, stream);
     if (rc) return rc;
@@ -558,6 +558,10 @@ int Plan::enqueue(const std::vector<Launch> &L, const double *dW, double *dY, in
 
 int Plan::read_workspaces(int nrhs, const int32_t *wsko, double *wskel, const int32_t *usko, double *uskel)
 {
+    if (precision != MXB_PREC_FP64) {
+        set_error("skeleton workspaces are kept by FP64 plans only");
+        return MXB_ERR_UNSUPPORTED;
+    }
     if (!dWskel || scratch_elems < (size_t)skel_total * nrhs) {
         set_error("no evaluation with this nrhs has run on the plan");
         return MXB_ERR_ARG;

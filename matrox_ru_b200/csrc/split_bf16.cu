@@ -1286,6 +1286,17 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
     }
     end_op();
 
+    // the split path reads only the tiled pools: release the FP64 copies of the CDS
+    const uint64_t fp64_len[3] = {D_len, B_len, VT_len};
+    double **fp64_buf[3] = {&dD, &dB, &dVT};
+    for (int q = 0; q < 3; ++q) {
+        if (!*fp64_buf[q]) continue;
+        cudaFree(*fp64_buf[q]);
+        allocations.erase(std::remove(allocations.begin(), allocations.end(), (void *)*fp64_buf[q]),
+                          allocations.end());
+        *fp64_buf[q] = nullptr;
+        device_bytes -= std::max<uint64_t>(fp64_len[q], 1) * sizeof(double);
+    }
     int rc = alloc((void **)&S->dErr, sizeof(int));
     if (rc) return rc;
     if (cudaMemset(S->dErr, 0, sizeof(int)) != cudaSuccess) {

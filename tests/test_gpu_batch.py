@@ -74,3 +74,37 @@ def test_batch_accumulates(torch):
     batch.status()
     for o, want in zip(outs, wants):
         assert np.linalg.norm(o.cpu().numpy() - want) / np.linalg.norm(want) <= 1e-5
+
+
+def c3_like_cases(count, seed):
+    """BASELINE config 3's recipe with N scaled down: N log-uniform, d from {8, 18, 28, 54},
+    Gaussian (h in [0.5, 3]) or inverse multiquadric kernels, nrhs log-uniform in [32, 512]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(np.exp(rng.uniform(np.log(512), np.log(2048))))
+        d = int(rng.choice([8, 18, 28, 54]))
+        kind = "gaussian" if rng.uniform() < 0.5 else "imq"
+        h = float(rng.uniform(0.5, 3.0))
+        X = S.gaussian_mixture(n, d, 8, -2.0, 2.0, 0.3, 1.0, seed=seed * 1000 + i)
+        cds = S.build_cds(X, S.KernelSpec(kind, h), leaf_size=128, budget=0.25, tol=1e-5, max_rank=64, seed=i)
+        r = int(np.exp(rng.uniform(np.log(32), np.log(512))))
+        out.append((cds, r))
+    return out
+
+
+def test_sixty_four_uneven_matrices_one_sequence(torch):
+    cases = c3_like_cases(64, seed=9)
+    plans = [H.Plan(c, "split_bf16") for c, _ in cases]
+    batch = H.Batch(plans)
+    per_plan = max(p.info()["launches"] for p in plans)
+    assert batch.info()["launches"] <= per_plan + 2  # merged by level, not 64 sequences
+    TWs, wants = [], []
+    for k, (c, r) in enumerate(cases):
+        TW = np.random.default_rng(k).standard_normal(c.n * r)
+        TWs.append(torch.as_tensor(TW, device="cuda"))
+        wants.append(O.eval_h2b(c, TW, r))
+    outs = batch.evaluate(TWs, [r for _, r in cases])
+    batch.status()
+    errs = [np.linalg.norm(o.cpu().numpy() - w) / np.linalg.norm(w) for o, w in zip(outs, wants)]
+    assert max(errs) <= 1e-5, max(errs)
