@@ -264,10 +264,12 @@ def main():
         torch.cuda.synchronize()
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
         with ClockSampler(local) as cs:
+            torch.cuda.nvtx.range_push("timed")  # lets a profiler select the timed launches
             for e0, e1 in ev:
                 e0.record(stream)
                 plan.evaluate(TW, r, out=out)
                 e1.record(stream)
+            torch.cuda.nvtx.range_pop()
             torch.cuda.synchronize()
         if dist:
             dist.barrier()
@@ -279,10 +281,24 @@ def main():
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ms = float(t.item())
         info = plan.info()
+        # launch-by-launch device times of one more evaluation (CUDA events on this stream)
+        prof = plan.profile(TW, r, out=out)
+        phases = {}
+        for x in prof:
+            ph = phases.setdefault(x["phase"], {"launches": 0, "ms": 0.0, "flops": 0.0, "issued_flops": 0.0})
+            ph["launches"] += 1
+            for key in ("ms", "flops", "issued_flops"):
+                ph[key] += x[key]
+        for ph in phases.values():
+            ph["ms"] = round(ph["ms"], 4)
+        tc = [x for x in prof if x["phase"] != "split_w"]
         res = {"ms": round(ms, 4),
                "executed_tflops": round(exec_flops[mode] / (ms * 1e-3) / 1e12, 2), "gflops": round(flops / (ms * 1e-3) / 1e9, 1), "launches_per_eval": info["launches"],
                "device_bytes": info["device_bytes"], "step_ms_min": round(min(per), 4),
-               "step_ms_max": round(max(per), 4), "clocks": cs.summary()}
+               "step_ms_max": round(max(per), 4), "clocks": cs.summary(),
+               "gemm_launches": len(tc), "gemm_ms": round(sum(x["ms"] for x in tc), 4),
+               "gemm_issued_flops": sum(x["issued_flops"] for x in tc), "phases": phases,
+               "launch_profile": [[x["phase"], x["level"], x["width"], round(x["ms"], 4)] for x in prof]}
         # accuracy on this CDS: vs the reference's FP64 evaluation (16-column slice) and vs dense
         if rank == 0:
             sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -316,18 +332,24 @@ def main():
 
     # roofline of the dominant kernel (the grouped GEMM: every launch of an evaluation)
     traffic = profile_traffic().get(best)
+    # achieved = flops per launch / mean launch time of the grouped-GEMM kernel, both from the
+    # launch-by-launch CUDA-event profile of one evaluation
+    nl, gms = max(head["gemm_launches"], 1), head["gemm_ms"]
     if best == "fp64":
-        roof = {"bound": "tensor", "achieved": round(flops / (ms * 1e-3) / 1e12, 3), "peak": round(fp64_peak, 2),
+        roof = {"bound": "tensor", "achieved": round(flops / (gms * 1e-3) / 1e12, 3), "peak": round(fp64_peak, 2),
                 "unit": "TFLOP/s", "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 (torch.matmul f64)",
-                "kernel": "gemm_f64_kernel (all launches of one evaluation)",
-                "per_launch_flops": flops // max(head["launches_per_eval"], 1)}
+                "kernel": "gemm_f64_kernel", "flops_counted": "algorithmic FP64 flops (computeFlops)",
+                "per_launch_flops": flops // nl}
     else:
-        roof = {"bound": "tensor", "achieved": round(exec_flops[best] / (ms * 1e-3) / 1e12, 3),
+        roof = {"bound": "tensor", "achieved": round(exec_flops[best] / (gms * 1e-3) / 1e12, 3),
                 "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
                 "peak_source": f"MEASURED_PEAKS.json bf16_tflops ({peak_src}, burst)",
-                "kernel": "tc_gemm_kernel + split kernels (all launches of one evaluation)",
-                "flops_counted": "executed bf16 tensor flops (3 or 6 products per algorithmic product)",
-                "per_launch_flops": exec_flops[best] // max(head["launches_per_eval"], 1)}
+                "kernel": "tc_gemm_kernel (tcgen05)",
+                "flops_counted": "bf16 tensor products of the algorithmic flops (3 or 6 per product), no padding",
+                "per_launch_flops": exec_flops[best] // nl,
+                "issued_tflops": round(head["gemm_issued_flops"] / (gms * 1e-3) / 1e12, 3)}
+    roof.update(launches=head["gemm_launches"], mean_launch_ms=round(gms / nl, 5),
+                whole_evaluation_tflops=round((flops if best == "fp64" else exec_flops[best]) / (ms * 1e-3) / 1e12, 3))
     roof["frac"] = round(roof["achieved"] / roof["peak"], 4)
     roof["traffic"] = traffic
 

@@ -256,6 +256,37 @@ MXB_API int32_t mxb_batch_info(const mxb_batch *batch, int32_t *launches, int32_
                                int32_t *nwidths);
 MXB_API int32_t mxb_batch_destroy(mxb_batch *batch);
 
+/* ---- per-launch timing (no counterpart in the reference, which times the whole HGEMM
+ * call with omp_get_wtime in matroxTest-V1/main.cpp:94-108) ----
+ * Evaluates Y = K~W (overwriting Y) once through the ordinary path, then twice launch by launch
+ * outside any graph, bracketing every launch with CUDA events on `stream`, and reports the
+ * second pass.  The launches are the ones the evaluation graph holds, in order, so Y on return
+ * is the ordinary result.  The call synchronises `stream`. */
+#define MXB_PHASE_SPLIT_W 0        /* W -> bf16 operand tiles (split-BF16 plans) */
+#define MXB_PHASE_UP 1             /* leaf projection (level 0) or transfer at height `level` */
+#define MXB_PHASE_FAR 2            /* far couplings into the nodes at depth `level` */
+#define MXB_PHASE_DOWN 3           /* downward transfer into the nodes at depth `level` */
+#define MXB_PHASE_NEAR 4           /* near field */
+#define MXB_PHASE_LEAF_DOWN 5      /* leaf downward projection into Y */
+#define MXB_PHASE_FAR_DOWN 6       /* FP64 plans: far + downward transfer, depth `level` */
+#define MXB_PHASE_NEAR_LEAF_DOWN 7 /* FP64 plans: near field + leaf downward projection */
+typedef struct mxb_op_profile {
+    int32_t phase;        /* MXB_PHASE_* */
+    int32_t level;        /* height or depth, see the phase */
+    int32_t width;        /* right-hand sides per work unit (0: no tensor-core work) */
+    int32_t units;        /* work units: output row tile x column tile */
+    double flops;         /* algorithmic flops, 2 m k n summed over the launch's products */
+    double issued_flops;  /* tensor-pipe flops issued: padded tiles, x3 / x6 for split products */
+    float ms;             /* device time of the launch */
+    int32_t pad;
+} mxb_op_profile;
+/* `*nops` receives the number of launches; at most `cap` records are written. */
+MXB_API int32_t mxb_plan_profile(mxb_plan *plan, const double *dW, double *dY, int32_t nrhs, void *stream,
+                                 mxb_op_profile *out, int32_t cap, int32_t *nops);
+MXB_API int32_t mxb_batch_profile(mxb_batch *batch, const double *const *dW, double *const *dY,
+                                  const int32_t *nrhs, void *stream, mxb_op_profile *out, int32_t cap,
+                                  int32_t *nops);
+
 /* ---- evaluation without device allocation ------------------------------------------------ */
 
 /* No counterpart in the reference (its evaluator runs on the host).  For callers that may

@@ -26,6 +26,8 @@ PREC_SPLIT_BF16_X6 = 3
 FLAG_MIRROR_WORKSPACES = 1
 FLAG_OUTPUT_IS_ZERO = 2
 DEBUG_STALL_ONE_WAIT = 1
+PHASES = {0: "split_w", 1: "up", 2: "far", 3: "down", 4: "near", 5: "leaf_down", 6: "far_down",
+          7: "near_leaf_down"}
 
 P = ctypes.c_void_p
 I32 = ctypes.c_int32
@@ -51,6 +53,12 @@ class CdsDesc(ctypes.Structure):
         ("npairx", P), ("npairy", P), ("ncount", I32),
         ("fpairx", P), ("fpairy", P), ("fcount", I32),
     ]
+
+
+class OpProfile(ctypes.Structure):
+    _fields_ = [("phase", I32), ("level", I32), ("width", I32), ("units", I32),
+                ("flops", ctypes.c_double), ("issued_flops", ctypes.c_double), ("ms", ctypes.c_float),
+                ("pad", I32)]
 
 
 _REF_ARGS_H2B = [P] * 12 + [I32] + [P] * 9 + [P] * 8  # up to fpairy
@@ -92,6 +100,9 @@ def load(path: str = LIB_PATH):
     lib.mxb_batch_status.argtypes = [P]
     lib.mxb_batch_info.argtypes = [P, ctypes.POINTER(I32), ctypes.POINTER(I32), I32, ctypes.POINTER(I32)]
     lib.mxb_batch_destroy.argtypes = [P]
+    lib.mxb_plan_profile.argtypes = [P, P, P, I32, P, ctypes.POINTER(OpProfile), I32, ctypes.POINTER(I32)]
+    lib.mxb_batch_profile.argtypes = [P, ctypes.POINTER(P), ctypes.POINTER(P), ctypes.POINTER(I32), P,
+                                      ctypes.POINTER(OpProfile), I32, ctypes.POINTER(I32)]
     lib.mxb_plan_set_test_hooks.argtypes = [P, I32, I64]
     lib.mxb_permute_rows.argtypes = [P, P, P, I32, I64, P, P, I64, I64, I32, I32, I32, P]
     lib.mxb_transform.argtypes = [P, P, P, I32, P, I64, I64, I32, P]

@@ -798,6 +798,28 @@ int32_t mxb_batch_evaluate(mxb_batch *batch, const double *const *dW, double *co
     return batch_evaluate(reinterpret_cast<Batch *>(batch), dW, dY, nrhs, accumulate, (cudaStream_t)stream);
 }
 
+int32_t mxb_plan_profile(mxb_plan *plan, const double *dW, double *dY, int32_t nrhs, void *stream,
+                         mxb_op_profile *out, int32_t cap, int32_t *nops)
+{
+    if (!plan) {
+        set_error("null plan");
+        return MXB_ERR_ARG;
+    }
+    int n = 0;
+    const int rc = static_cast<Plan *>(plan)->profile(dW, dY, nrhs, (cudaStream_t)stream, out, cap, &n);
+    if (nops) *nops = n;
+    return rc;
+}
+
+int32_t mxb_batch_profile(mxb_batch *batch, const double *const *dW, double *const *dY, const int32_t *nrhs,
+                          void *stream, mxb_op_profile *out, int32_t cap, int32_t *nops)
+{
+    int n = 0;
+    const int rc = batch_profile(reinterpret_cast<Batch *>(batch), dW, dY, nrhs, (cudaStream_t)stream, out, cap, &n);
+    if (nops) *nops = n;
+    return rc;
+}
+
 int32_t mxb_batch_status(mxb_batch *batch) { return batch_status(reinterpret_cast<Batch *>(batch)); }
 
 int32_t mxb_batch_info(const mxb_batch *batch, int32_t *launches, int32_t *widths, int32_t cap, int32_t *nwidths)

@@ -48,7 +48,8 @@ struct Launch {
     int32_t task0;
     int32_t ntasks;
     int32_t max_m;   // largest M of the launch (row tile count is implied by tasks)
-    int32_t kind;    // phase id, for profiling labels
+    int32_t kind;    // MXB_PHASE_* of the launch, for profiling
+    int32_t level;   // height (up) or depth (far + down)
 };
 
 // Device pointers an evaluation needs; passed by value to every kernel.

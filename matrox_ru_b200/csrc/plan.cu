@@ -240,10 +240,11 @@ void Plan::build_tasks(int tile)
     tasks.clear();
     launches_fwd.clear();
     launches_adj.clear();
-    auto begin_launch = [&](std::vector<Launch> &L, int kind) {
+    auto begin_launch = [&](std::vector<Launch> &L, int kind, int level) {
         Launch l{};
         l.task0 = (int)tasks.size();
         l.kind = kind;
+        l.level = level;
         L.push_back(l);
     };
     auto end_launch = [&](std::vector<Launch> &L) {
@@ -271,7 +272,7 @@ void Plan::build_tasks(int tile)
     // phases 1-2: up-sweep, shared by forward and adjoint
     std::vector<Launch> up;
     for (int h = 0; h <= maxh; ++h) {
-        begin_launch(up, h == 0 ? 1 : 2);
+        begin_launch(up, MXB_PHASE_UP, h);
         for (int v : bfs) {
             if (height[v] != h || !projects(v)) continue;
             const int s = slen[v];
@@ -305,7 +306,7 @@ void Plan::build_tasks(int tile)
     for (int adj = 0; adj < 2; ++adj) {
         std::vector<Launch> &L = adj ? launches_adj : launches_fwd;
         for (int dd = 1; dd <= maxd; ++dd) {
-            begin_launch(L, 3);
+            begin_launch(L, MXB_PHASE_FAR_DOWN, dd);
             for (int c : bfs) {
                 if (depth[c] != dd || !projects(c)) continue;
                 const int item0 = (int)items.size();
@@ -328,7 +329,7 @@ void Plan::build_tasks(int tile)
             end_launch(L);
         }
         // phase 4: near + leaf down
-        begin_launch(L, 4);
+        begin_launch(L, MXB_PHASE_NEAR_LEAF_DOWN, 0);
         for (int v : bfs) {
             if (lch[v] != -1) continue;
             const int x = lm[v];
@@ -554,6 +555,56 @@ int Plan::enqueue(const std::vector<Launch> &L, const double *dW, double *dY, in
         }
     }
     return MXB_OK;
+}
+
+// Launch-by-launch timing of the forward evaluation (mxb_plan_profile).
+int Plan::profile(const double *dW, double *dY, int nrhs, cudaStream_t stream, mxb_op_profile *out, int cap,
+                  int *nops)
+{
+    int rc = run(launches_fwd, dW, dY, nrhs, nullptr, nullptr, 0, stream);  // checks, offsets, graphs, tuning
+    if (rc) return rc;
+    if (precision != MXB_PREC_FP64) return batch_profile(split_bf16_batch(*this), &dW, &dY, &nrhs, stream, out, cap, nops);
+    const std::vector<Launch> &L = launches_fwd;
+    const int tile = row_tile_for(precision), ncol = (int)((nrhs + tile - 1) / tile);
+    std::vector<cudaEvent_t> ev(L.size() + 1, nullptr);
+    for (cudaEvent_t &e : ev)
+        if (!rc && cudaEventCreate(&e) != cudaSuccess) {
+            set_error("profile: creating CUDA events failed");
+            rc = MXB_ERR_CUDA;
+        }
+    for (int rep = 0; rep < 2 && !rc; ++rep) {
+        cudaEventRecord(ev[0], stream);
+        for (size_t i = 0; i < L.size() && !rc; ++i) {
+            rc = enqueue(std::vector<Launch>{L[i]}, dW, dY, nrhs, 0, stream);
+            cudaEventRecord(ev[i + 1], stream);
+        }
+        if (!rc && cudaStreamSynchronize(stream) != cudaSuccess) {
+            set_error("profile: stream synchronisation failed");
+            rc = MXB_ERR_CUDA;
+        }
+    }
+    if (nops) *nops = (int)L.size();
+    for (size_t i = 0; i < L.size() && !rc && (int)i < cap && out; ++i) {
+        const Launch &l = L[i];
+        mxb_op_profile &o = out[i];
+        o = mxb_op_profile{};
+        o.phase = l.kind;
+        o.level = l.level;
+        o.width = tile;
+        o.units = l.ntasks * ncol;
+        for (int t = l.task0; t < l.task0 + l.ntasks; ++t) {
+            const Task &T = tasks[t];
+            const double rows = std::min(tile, T.M - T.m0);
+            for (int k = T.item0; k < T.item0 + T.nitem; ++k) {
+                o.flops += 2.0 * rows * items[k].K * nrhs;
+                o.issued_flops += 2.0 * tile * items[k].K * (double)ncol * tile;
+            }
+        }
+        cudaEventElapsedTime(&o.ms, ev[i], ev[i + 1]);
+    }
+    for (cudaEvent_t e : ev)
+        if (e) cudaEventDestroy(e);
+    return rc;
 }
 
 int Plan::read_workspaces(int nrhs, const int32_t *wsko, double *wskel, const int32_t *usko, double *uskel)

@@ -62,6 +62,8 @@ struct Plan : public mxb_plan {
     int stage_offsets(int slot, const int32_t *ofs, int nrhs, cudaStream_t stream);
     int run(const std::vector<Launch> &L, const double *dW, double *dY, int nrhs, const int32_t *wofs,
             const int32_t *yofs, int accumulate, cudaStream_t stream);
+    int profile(const double *dW, double *dY, int nrhs, cudaStream_t stream, mxb_op_profile *out, int cap,
+                int *nops);
     int read_workspaces(int nrhs, const int32_t *wsko, double *wskel, const int32_t *usko, double *uskel);
     uint64_t flops(int nrhs) const;
 
@@ -99,5 +101,8 @@ void batch_destroy(Batch *b);
 int batch_launches(const Batch *b);
 int batch_tuned_widths(const Batch *b, int *widths, int cap);
 int split_bf16_status(Plan &p);
+Batch *split_bf16_batch(Plan &p);  // the plan's own single-plan batch
+int batch_profile(Batch *b, const double *const *W, double *const *Y, const int *nrhs, cudaStream_t stream,
+                  mxb_op_profile *out, int cap, int *nops);
 
 }  // namespace mxb

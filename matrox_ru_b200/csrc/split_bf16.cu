@@ -64,7 +64,7 @@ struct TcItem {
     uint64_t a_off;   // byte offset of A's tile (0, 0) in the plan's A pool of the launch
     int64_t b_base;   // K-tile base of the B operand's node / leaf in the B buffer
     int32_t KT;       // K tiles of this item
-    int32_t pad;
+    int32_t K;        // K before padding to whole tiles (flop accounting)
 };
 
 // Output of a tensor-core task.
@@ -607,7 +607,7 @@ int64_t op_key(int phase, int level)
 
 struct Op {             // one op of one plan
     int64_t key;
-    int phase, P;
+    int phase, level, P;
     int a_pool, b_buf, t_buf;
     int first, count;   // range in the plan's tasks (TC) or jobs (W split)
 };
@@ -644,7 +644,7 @@ struct Batch : public mxb_batch {
     std::vector<Plan *> plans;
     struct MOp {
         int64_t key;
-        int phase, P, a_pool, b_buf, t_buf;
+        int phase, level, P, a_pool, b_buf, t_buf;
         int first, count;  // range in the merged tasks or jobs
         int max_kt;
     };
@@ -700,6 +700,10 @@ struct Batch : public mxb_batch {
                 int only_op = -1);
     int units_for(Entry &e, const std::vector<int> &bn);
     int tune(Entry &e, std::vector<PlanArgs> pa, std::vector<int> &bn, cudaStream_t stream, long long wait_cycles);
+    Entry *find(const double *const *W, double *const *Y, const std::vector<int> &nr, int accumulate,
+                int debug_flags);
+    int profile(const double *const *W, double *const *Y, const int *nrhs, cudaStream_t stream, mxb_op_profile *out,
+                int cap, int *nops);
 };
 
 int Batch::build(const std::vector<Plan *> &ps)
@@ -722,6 +726,7 @@ int Batch::build(const std::vector<Plan *> &ps)
         m.key = kv.first;
         const Op *o0 = kv.second[0].second;
         m.phase = o0->phase;
+        m.level = o0->level;
         m.P = o0->P;
         m.a_pool = o0->a_pool;
         m.b_buf = o0->b_buf;
@@ -978,12 +983,7 @@ int Batch::evaluate(const double *const *W, double *const *Y, const int *nrhs, i
     }
     if (realloc) clear();
     MXB_CUDA_OR(configure_all_tc());
-    Entry *hit = nullptr;
-    for (Entry &e : entries) {
-        bool same = e.accumulate == accumulate && e.nrhs == nr && e.debug_flags == debug_flags;
-        for (int i = 0; same && i < np; ++i) same = e.W[i] == W[i] && e.Y[i] == Y[i];
-        if (same) hit = &e;
-    }
+    Entry *hit = find(W, Y, nr, accumulate, debug_flags);
     if (!hit) {
         if (entries.size() >= 8) {
             release(entries.front());
@@ -1067,6 +1067,73 @@ int Batch::evaluate(const double *const *W, double *const *Y, const int *nrhs, i
     }
     MXB_CUDA_OR(cudaGraphLaunch(hit->exec, stream));
     return MXB_OK;
+}
+
+Batch::Entry *Batch::find(const double *const *W, double *const *Y, const std::vector<int> &nr, int accumulate,
+                          int debug_flags)
+{
+    Entry *hit = nullptr;
+    for (Entry &e : entries) {
+        bool same = e.accumulate == accumulate && e.nrhs == nr && e.debug_flags == debug_flags;
+        for (size_t i = 0; same && i < plans.size(); ++i) same = e.W[i] == W[i] && e.Y[i] == Y[i];
+        if (same) hit = &e;
+    }
+    return hit;
+}
+
+// Launch-by-launch timing of one evaluation (mxb_batch_profile / mxb_plan_profile); the
+// evaluation graph of these operands has been built (and run) by the caller.
+int Batch::profile(const double *const *W, double *const *Y, const int *nrhs, cudaStream_t stream, mxb_op_profile *out,
+                   int cap, int *nops)
+{
+    const std::vector<int> nr(nrhs, nrhs + plans.size());
+    Entry *e = find(W, Y, nr, 0, 0);
+    if (!e) return batch_fail("profile: no evaluation graph for these operands");
+    std::vector<cudaEvent_t> ev(ops.size() + 1, nullptr);
+    int rc = MXB_OK;
+    for (cudaEvent_t &x : ev)
+        if (!rc && cudaEventCreate(&x) != cudaSuccess) rc = batch_fail("profile: creating CUDA events failed", MXB_ERR_CUDA);
+    for (int rep = 0; rep < 2 && !rc; ++rep) {
+        cudaEventRecord(ev[0], stream);
+        for (size_t k = 0; k < ops.size() && !rc; ++k) {
+            rc = enqueue(*e, stream, 0, 0, e->bn, (int)k);
+            cudaEventRecord(ev[k + 1], stream);
+        }
+        if (!rc && cudaStreamSynchronize(stream) != cudaSuccess)
+            rc = batch_fail("profile: stream synchronisation failed", MXB_ERR_CUDA);
+    }
+    if (nops) *nops = (int)ops.size();
+    std::vector<TcUnit> units;
+    if (!rc) {
+        size_t n = 0;
+        for (int c : e->unit_count) n += (size_t)c;
+        units.resize(n);
+        if (n && cudaMemcpy(units.data(), e->dUnits, n * sizeof(TcUnit), cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = batch_fail("profile: reading the work units failed", MXB_ERR_CUDA);
+    }
+    for (size_t k = 0; k < ops.size() && !rc && (int)k < cap && out; ++k) {
+        const MOp &m = ops[k];
+        mxb_op_profile &o = out[k];
+        o = mxb_op_profile{};
+        o.phase = m.phase;
+        o.level = m.level;
+        o.width = e->bn[k];
+        o.units = e->unit_count[k];
+        const double products = m.P == 2 ? 3.0 : 6.0;
+        for (int u = e->unit_first[k]; u < e->unit_first[k] + e->unit_count[k]; ++u) {
+            const TcTask &t = tasks[units[u].task];
+            const double rows = std::min(128, t.M - t.m0);
+            const double cols = std::min(o.width, nr[t.plan] - units[u].col * o.width);
+            for (int q = t.item0; q < t.item0 + t.nitem; ++q) {
+                o.flops += 2.0 * rows * items[q].K * cols;
+                o.issued_flops += products * 2.0 * 128 * (64.0 * items[q].KT) * o.width;
+            }
+        }
+        cudaEventElapsedTime(&o.ms, ev[k], ev[k + 1]);
+    }
+    for (cudaEvent_t x : ev)
+        if (x) cudaEventDestroy(x);
+    return rc;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1174,6 +1241,7 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
         Op o{};
         o.key = op_key(phase, level);
         o.phase = phase;
+        o.level = level;
         o.P = P;
         o.a_pool = a_pool;
         o.b_buf = b_buf;
@@ -1208,6 +1276,7 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
         it.a_off = a_off;
         it.b_base = b_base;
         it.KT = KT(K);
+        it.K = K;
         if (it.KT > 0) S->items.push_back(it);
     };
 
@@ -1327,6 +1396,8 @@ int split_bf16_prepare() { return configure_all_tc() == cudaSuccess ? MXB_OK : M
 
 int split_bf16_launches(const Plan &p) { return p.bf16 ? (int)p.bf16->self->ops.size() : 0; }
 
+Batch *split_bf16_batch(Plan &p) { return p.bf16 ? p.bf16->self : nullptr; }
+
 int split_bf16_status(Plan &p)
 {
     if (!p.bf16) return MXB_OK;
@@ -1373,6 +1444,15 @@ int batch_evaluate(Batch *b, const double *const *W, double *const *Y, const int
         if (rc) return rc;
     }
     return b->evaluate(W, Y, nrhs, accumulate, stream, 0, 0);
+}
+
+int batch_profile(Batch *b, const double *const *W, double *const *Y, const int *nrhs, cudaStream_t stream,
+                  mxb_op_profile *out, int cap, int *nops)
+{
+    if (!b || !W || !Y || !nrhs) return batch_fail("bad batch arguments");
+    int rc = batch_evaluate(b, W, Y, nrhs, 0, stream);  // builds the entry (and tunes) if needed
+    if (rc) return rc;
+    return b->profile(W, Y, nrhs, stream, out, cap, nops);
 }
 
 int batch_status(Batch *b)

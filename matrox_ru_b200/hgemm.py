@@ -192,6 +192,11 @@ def cds_desc(cds, keep: list) -> _lib.CdsDesc:
     return d
 
 
+def _profile_records(recs, n):
+    return [{"phase": _lib.PHASES.get(r.phase, str(r.phase)), "level": r.level, "width": r.width, "units": r.units,
+             "flops": r.flops, "issued_flops": r.issued_flops, "ms": r.ms} for r in recs[:min(n, len(recs))]]
+
+
 class Plan:
     """Device-resident CDS and task lists (``mxb_plan_*``)."""
 
@@ -258,6 +263,20 @@ class Plan:
                                             int(accumulate), _stream_ptr(stream)), "mxb_plan_evaluate")
         return out
 
+    def profile(self, TW, nrhs: int, out=None, stream=None):
+        """out = K~ TW, then the device time and flops of every launch of one evaluation
+        (``mxb_plan_profile``): a list of dicts in launch order."""
+        torch = _torch()
+        self._check_operand(TW, nrhs)
+        if out is None:
+            out = torch.zeros(self.n * nrhs, dtype=torch.float64, device=TW.device)
+        self._check_operand(out, nrhs)
+        recs = (_lib.OpProfile * 4096)()
+        n = I32()
+        check(_lib.load().mxb_plan_profile(self._h, TW.data_ptr(), out.data_ptr(), nrhs, _stream_ptr(stream),
+                                           recs, 4096, ctypes.byref(n)), "mxb_plan_profile")
+        return _profile_records(recs, n.value)
+
     def adjoint(self, TG, nrhs: int, out=None, accumulate: bool = False, stream=None):
         """out (+)= K~^T TG (packed leaf-blocked float64 CUDA tensors)."""
         torch = _torch()
@@ -317,6 +336,18 @@ class Batch:
 
     def status(self) -> None:
         check(_lib.load().mxb_batch_status(self._h), "mxb_batch_status")
+
+    def profile(self, TWs, nrhs, outs, stream=None):
+        """outs[i] = K~_i TWs[i], then the device time and flops of every merged launch."""
+        n = len(self.plans)
+        W = (P * n)(*[t.data_ptr() for t in TWs])
+        Y = (P * n)(*[o.data_ptr() for o in outs])
+        R = (I32 * n)(*[int(r) for r in nrhs])
+        recs = (_lib.OpProfile * 4096)()
+        cnt = I32()
+        check(_lib.load().mxb_batch_profile(self._h, W, Y, R, _stream_ptr(stream), recs, 4096, ctypes.byref(cnt)),
+              "mxb_batch_profile")
+        return _profile_records(recs, cnt.value)
 
     def info(self):
         l, nw = I32(), I32()
