@@ -298,7 +298,8 @@ def main():
                "step_ms_max": round(max(per), 4), "clocks": cs.summary(),
                "gemm_launches": len(tc), "gemm_ms": round(sum(x["ms"] for x in tc), 4),
                "gemm_issued_flops": sum(x["issued_flops"] for x in tc), "phases": phases,
-               "launch_profile": [[x["phase"], x["level"], x["width"], round(x["ms"], 4)] for x in prof]}
+               "launch_profile": [[x["phase"], x["level"], x["width"], "pair" if x["pair"] else "cta",
+                                   round(x["ms"], 4)] for x in prof]}
         # accuracy on this CDS: vs the reference's FP64 evaluation (16-column slice) and vs dense
         if rank == 0:
             sys.path.insert(0, os.path.join(ROOT, "oracle"))

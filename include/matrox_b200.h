@@ -251,7 +251,10 @@ MXB_API int32_t mxb_batch_evaluate(mxb_batch *batch, const double *const *dW, do
                                    const int32_t *nrhs, int32_t accumulate, void *stream);
 /* Synchronises and reports a kernel-side failure (MXB_ERR_TIMEOUT) of any plan; clears it. */
 MXB_API int32_t mxb_batch_status(mxb_batch *batch);
-/* Launches per evaluation and the tuned column-tile widths of the last evaluation. */
+/* Launches per evaluation and the tuned tile of every tensor-core launch of the last
+ * evaluation: the column-tile width, plus MXB_TILE_PAIR when the launch runs on pairs of SMs
+ * (a 2-CTA cluster computing 256-row tiles with tcgen05.mma.cta_group::2). */
+#define MXB_TILE_PAIR 4096
 MXB_API int32_t mxb_batch_info(const mxb_batch *batch, int32_t *launches, int32_t *widths, int32_t cap,
                                int32_t *nwidths);
 MXB_API int32_t mxb_batch_destroy(mxb_batch *batch);
@@ -278,7 +281,7 @@ typedef struct mxb_op_profile {
     double flops;         /* algorithmic flops, 2 m k n summed over the launch's products */
     double issued_flops;  /* tensor-pipe flops issued: padded tiles, x3 / x6 for split products */
     float ms;             /* device time of the launch */
-    int32_t pad;
+    int32_t pair;         /* 1: runs on pairs of SMs (256-row tiles) */
 } mxb_op_profile;
 /* `*nops` receives the number of launches; at most `cap` records are written. */
 MXB_API int32_t mxb_plan_profile(mxb_plan *plan, const double *dW, double *dY, int32_t nrhs, void *stream,

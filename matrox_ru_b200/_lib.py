@@ -26,6 +26,7 @@ PREC_SPLIT_BF16_X6 = 3
 FLAG_MIRROR_WORKSPACES = 1
 FLAG_OUTPUT_IS_ZERO = 2
 DEBUG_STALL_ONE_WAIT = 1
+TILE_PAIR = 4096
 PHASES = {0: "split_w", 1: "up", 2: "far", 3: "down", 4: "near", 5: "leaf_down", 6: "far_down",
           7: "near_leaf_down"}
 
@@ -58,7 +59,7 @@ class CdsDesc(ctypes.Structure):
 class OpProfile(ctypes.Structure):
     _fields_ = [("phase", I32), ("level", I32), ("width", I32), ("units", I32),
                 ("flops", ctypes.c_double), ("issued_flops", ctypes.c_double), ("ms", ctypes.c_float),
-                ("pad", I32)]
+                ("pair", I32)]
 
 
 _REF_ARGS_H2B = [P] * 12 + [I32] + [P] * 9 + [P] * 8  # up to fpairy

@@ -130,6 +130,7 @@ struct LaunchArgs {
     int nunits;
     int a_pool, b_buf, t_buf;
     int stall_test;         // test hook: CTA 0 withholds its first stage, so a wait runs out
+    int kchain;             // K tiles accumulated per TMEM accumulator fill (1 or 2)
 };
 
 // ---------------------------------------------------------------------------------------
@@ -226,10 +227,15 @@ __device__ __forceinline__ void transpose8(float (&x)[8], int lane)
     }
 }
 
-template <int P, int BN, int STAGES_>
+// Launch shape.  PAIR: a cluster of two CTAs (one per SM) computes a 256-row x BN tile with
+// tcgen05.mma.cta_group::2; each CTA stages its own 128 rows of A and half of the BN rows of
+// B, so a pair moves a third less operand data per flop than two single CTAs and has room for
+// a deeper pipeline.
+template <int P, int BN, int STAGES_, bool PAIR = false>
 struct TcCfg {
     static constexpr int STAGES = STAGES_;
-    static constexpr int B_ROWS_BYTES = BN * 128;           // one part of the B operand, BN rows
+    static constexpr int B_ROWS = PAIR ? BN / 2 : BN;      // B rows (output columns) staged per CTA
+    static constexpr int B_ROWS_BYTES = B_ROWS * 128;      // one part of the staged B operand
     static constexpr int A_BYTES = P * TILE_BYTES;
     static constexpr int B_BYTES = P * B_ROWS_BYTES;
     static constexpr int STAGE = A_BYTES + B_BYTES;
@@ -238,53 +244,87 @@ struct TcCfg {
     static constexpr int EPI_WARPS = 8;          // two per TMEM lane quarter, one per column half
     static constexpr int THREADS = (EPI_WARPS + 2) * 32;
     static constexpr int COLS = BN / 2;          // accumulator columns per epilogue thread
-    static constexpr int TMEM_COLS = 2 * BN;     // two accumulator buffers
+    static constexpr int NACC = BN >= 256 ? 2 : 4;  // TMEM accumulator buffers (512 columns at most)
+    static constexpr int TMEM_COLS = NACC * BN;
+    static constexpr int M_MMA = PAIR ? 256 : 128;
     static_assert(SMEM <= 232448, "shared memory");
+    static_assert(B_ROWS % 64 == 0, "B rows per CTA");
 };
 
 // Tensor-core FP32 accumulation is not round-to-nearest: its error grows with the number of
 // MMAs chained into one accumulator (measured ~4e-5 relative after 8192-deep chains).  So
-// each 64-deep K tile gets a fresh TMEM accumulator (two buffers, alternating), and the
+// every 64-deep K tile (bf16x6 launches) or pair of K tiles (bf16x3 launches, whose split
+// error is ten times larger) gets a fresh TMEM accumulator (2 or 4 buffers in rotation), and the
 // epilogue warps add every tile's partial sums into per-thread FP32 registers with ordinary
-// round-to-nearest adds while the tensor core already works on the next tile.
+// round-to-nearest adds while the tensor core already works on the next tiles.
 //
-// Persistent: CTA b walks the units b, b + gridDim.x, ...  The three roles walk the same
+// Persistent: CTA (or CTA pair) b walks the units b, b + grid, ...  The roles walk the same
 // sequence, so one K-tile counter drives every stage and accumulator phase; TMEM and the
 // barriers are set up once, and the epilogue of one unit overlaps the MMAs of the next.
-template <int P, int BN, int STAGES_>
-__global__ void __launch_bounds__(TcCfg<P, BN, STAGES_>::THREADS, 1) tc_gemm_kernel(LaunchArgs la)
+//
+// In a pair the even CTA issues the MMAs.  The odd CTA's MMA-warp thread relays "my stage has
+// landed" to the even CTA's pfull barrier, its epilogue warps arrive on the even CTA's acce
+// barrier, and the even CTA's commits arrive on both CTAs' barriers.  A failed wait in either
+// CTA sets both CTAs' abort words.
+template <int P, int BN, int STAGES_, bool PAIR>
+__global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_gemm_kernel(LaunchArgs la)
 {
-    using C = TcCfg<P, BN, STAGES_>;
+    using C = TcCfg<P, BN, STAGES_, PAIR>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + C::STAGES * C::STAGE);
     uint64_t *empty = full + C::STAGES;
-    uint64_t *accf = empty + C::STAGES;  // accumulator buffer b holds a finished K tile
-    uint64_t *acce = accf + 2;           // accumulator buffer b has been drained
-    uint64_t *doneb = acce + 2;          // every MMA this CTA issued has completed
+    uint64_t *pfull = empty + C::STAGES;  // pair: the odd CTA's copy of the stage has landed
+    uint64_t *accf = pfull + C::STAGES;   // accumulator buffer b holds a finished K tile
+    uint64_t *acce = accf + C::NACC;      // accumulator buffer b has been drained
+    uint64_t *doneb = acce + C::NACC;     // every MMA of this CTA (pair) has completed
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(doneb + 1);
     volatile int *abort_word = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = PAIR ? tc::cluster_ctarank() : 0u;
+    const bool issuer = rank == 0;
+    const int unit0 = PAIR ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
+    const int ustride = PAIR ? (int)(gridDim.x >> 1) : (int)gridDim.x;
+    auto raise_abort = [&]() {
+        *abort_word = 1;
+        if constexpr (PAIR) tc::st_remote_u32(tc::peer_smem((const void *)abort_word, rank ^ 1u), 1u);
+    };
+    // waits on barriers that the other CTA of a pair completes take cluster-scope acquire
+    auto wait_x = [&](uint64_t *bar, uint32_t parity, volatile int *ab) {
+        if constexpr (PAIR) return tc::mbar_wait_cluster(bar, parity, ab, la.wait_cycles);
+        else return tc::mbar_wait(bar, parity, ab, la.wait_cycles);
+    };
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < C::STAGES; ++s) {
             tc::mbar_init(&full[s], 1);
             tc::mbar_init(&empty[s], 1);
+            tc::mbar_init(&pfull[s], 1);
         }
-        for (int b = 0; b < 2; ++b) {
+        for (int b = 0; b < C::NACC; ++b) {
             tc::mbar_init(&accf[b], 1);
-            tc::mbar_init(&acce[b], C::EPI_WARPS);
+            tc::mbar_init(&acce[b], C::EPI_WARPS * (PAIR ? 2 : 1));
         }
         tc::mbar_init(doneb, 1);
         *abort_word = 0;
         tc::fence_mbar_init();
     }
-    if (warp == 0) tc::tmem_alloc(tmem_slot, C::TMEM_COLS);
+    if (warp == 0) {
+        if constexpr (PAIR) tc::tmem_alloc_pair(tmem_slot, C::TMEM_COLS);
+        else tc::tmem_alloc(tmem_slot, C::TMEM_COLS);
+    }
     tc::fence_before_sync();
     __syncthreads();
+    if constexpr (PAIR) tc::cluster_sync();  // both CTAs' barriers and TMEM exist
     tc::fence_after_sync();
     const uint32_t tmem = *tmem_slot;
+
+    auto unit_ktiles = [&](const TcTask &t) {
+        int k = 0;
+        for (int q = 0; q < t.nitem; ++q) k += la.items[t.item0 + q].KT;
+        return k;
+    };
 
     if (warp == C::EPI_WARPS) {
         if (lane == 0) {
@@ -293,35 +333,41 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_>::THREADS, 1) tc_gemm_ker
             uint32_t filled[C::STAGES];   // rounds filled per stage (drained before exit)
 #pragma unroll
             for (int s = 0; s < C::STAGES; ++s) filled[s] = 0;
-            for (int u = blockIdx.x; u < la.nunits && !*abort_word; u += gridDim.x) {
+            for (int u = unit0; u < la.nunits && !*abort_word; u += ustride) {
                 const TcUnit un = la.units[u];
                 const TcTask t = la.tasks[un.task];
                 const PlanArgs *pa = la.plans + t.plan;
                 const uint8_t *a_pool = pa->pool[la.a_pool];
                 const uint8_t *b_pool = pa->buf[la.b_buf];
                 const int NT = pa->NT;
-                const int n0 = un.col * BN;
+                const int cb = un.col * BN + (int)rank * C::B_ROWS;  // first B row staged here
                 const TcItem *ti = la.items + t.item0;
-                const int mt = t.m0 / 128;
+                const int mt = t.m0 / 128 + (int)rank;
+                // the odd CTA's rows may lie past the block: its A tile does not exist, and the
+                // MMA rows it feeds are never stored
+                const bool a_ok = !PAIR || issuer || t.m0 + 128 < t.M;
+                const uint32_t tx = (a_ok ? C::A_BYTES : 0) + C::B_BYTES;
                 for (int q = 0; q < t.nitem && !*abort_word; ++q) {
                     const TcItem it = ti[q];
                     for (int kt = 0; kt < it.KT; ++kt, ++g) {
                         const int s = g % C::STAGES;
                         const uint32_t round = g / C::STAGES;
-                        if (!tc::mbar_wait(&empty[s], (round & 1) ^ 1, abort_word, la.wait_cycles)) {
-                            *abort_word = 1;
+                        if (!wait_x(&empty[s], (round & 1) ^ 1, abort_word)) {
+                            raise_abort();
                             break;
                         }
                         if (la.stall_test && blockIdx.x == 0 && g == 0) continue;  // never filled
                         uint8_t *sa = smem + s * C::STAGE;
                         uint8_t *sb = sa + C::A_BYTES;
-                        tc::mbar_expect_tx(&full[s], C::STAGE);
-                        const uint8_t *ga = a_pool + it.a_off + ((size_t)mt * it.KT + kt) * (size_t)P * TILE_BYTES;
-                        tc::bulk_g2s(sa, ga, C::A_BYTES, &full[s]);
-                        if (BN >= 128) {
+                        tc::mbar_expect_tx(&full[s], tx);
+                        if (a_ok) {
+                            const uint8_t *ga = a_pool + it.a_off + ((size_t)mt * it.KT + kt) * (size_t)P * TILE_BYTES;
+                            tc::bulk_g2s(sa, ga, C::A_BYTES, &full[s]);
+                        }
+                        if (C::B_ROWS >= 128) {
 #pragma unroll
-                            for (int hh = 0; hh < BN / 128; ++hh) {
-                                const size_t nt = (size_t)(n0 >> 7) + hh;
+                            for (int hh = 0; hh < C::B_ROWS / 128; ++hh) {
+                                const size_t nt = (size_t)(cb >> 7) + hh;
                                 const uint8_t *gb =
                                     b_pool + ((size_t)it.b_base * NT + nt * it.KT + kt) * 3 * (size_t)TILE_BYTES;
 #pragma unroll
@@ -330,12 +376,12 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_>::THREADS, 1) tc_gemm_ker
                                                  TILE_BYTES, &full[s]);
                             }
                         } else {
-                            // BN rows starting at row n0 % 128 of a 128-row tile: contiguous, and the
-                            // swizzle phase (row % 8) is unchanged by the 64-row offset
+                            // B_ROWS rows starting at row cb % 128 of a 128-row tile: contiguous, and
+                            // the swizzle phase (row % 8) is unchanged by the 64-row offset
                             const uint8_t *gb = b_pool +
-                                                ((size_t)it.b_base * NT + (size_t)(n0 >> 7) * it.KT + kt) * 3 *
+                                                ((size_t)it.b_base * NT + (size_t)(cb >> 7) * it.KT + kt) * 3 *
                                                     (size_t)TILE_BYTES +
-                                                (size_t)(n0 & 127) * 128;
+                                                (size_t)(cb & 127) * 128;
 #pragma unroll
                             for (int p = 0; p < P; ++p)
                                 tc::bulk_g2s(sb + p * C::B_ROWS_BYTES, gb + (size_t)p * TILE_BYTES, C::B_ROWS_BYTES,
@@ -354,89 +400,126 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_>::THREADS, 1) tc_gemm_ker
             }
         }
     } else if (warp == C::EPI_WARPS + 1) {
-        if (lane == 0) {
+        if (lane == 0 && issuer) {
             // ---------------- MMA issuer ----------------
-            constexpr uint32_t IDESC = tc::idesc_bf16_f32(128, BN);
+            constexpr uint32_t IDESC = tc::idesc_bf16_f32(C::M_MMA, BN);
             constexpr int PA[6] = {0, 0, 1, 0, 1, 2};
             constexpr int PB[6] = {0, 1, 0, 2, 1, 0};
-            uint32_t g = 0;
+            uint32_t g = 0;   // K-tile (stage) counter
+            uint32_t ga = 0;  // accumulator-fill counter
             bool any = false;
-            for (int u = blockIdx.x; u < la.nunits && !*abort_word; u += gridDim.x) {
-                const TcTask t = la.tasks[la.units[u].task];
-                int ktiles = 0;
-                for (int q = 0; q < t.nitem; ++q) ktiles += la.items[t.item0 + q].KT;
+            for (int u = unit0; u < la.nunits && !*abort_word; u += ustride) {
+                const int ktiles = unit_ktiles(la.tasks[la.units[u].task]);
                 for (int i = 0; i < ktiles; ++i, ++g) {
                     const int s = g % C::STAGES;
                     const uint32_t round = g / C::STAGES;
-                    const int b = g & 1;
-                    const uint32_t use = g >> 1;
-                    if (!tc::mbar_wait(&acce[b], (use & 1) ^ 1, abort_word, la.wait_cycles) ||
-                        !tc::mbar_wait(&full[s], round & 1, abort_word, la.wait_cycles)) {
-                        *abort_word = 1;
+                    const int b = ga % C::NACC;
+                    const uint32_t use = ga / C::NACC;
+                    const bool first = i % la.kchain == 0;
+                    const bool last = i % la.kchain == la.kchain - 1 || i == ktiles - 1;
+                    if ((first && !wait_x(&acce[b], (use & 1) ^ 1, abort_word)) ||
+                        !tc::mbar_wait(&full[s], round & 1, abort_word, la.wait_cycles) ||
+                        (PAIR && !wait_x(&pfull[s], round & 1, abort_word))) {
+                        raise_abort();
                         break;
                     }
                     tc::fence_after_sync();
                     const uint32_t sa = tc::smem_u32(smem + s * C::STAGE);
                     const uint32_t sb = sa + C::A_BYTES;
                     const uint32_t dst = tmem + (uint32_t)(b * BN);
-                    uint32_t accum = 0;
+                    uint32_t accum = first ? 0u : 1u;
 #pragma unroll
                     for (int ks = 0; ks < 4; ++ks) {
 #pragma unroll
                         for (int j = 0; j < C::NPROD; ++j) {
                             const uint64_t ad = tc::smem_desc_sw128(sa + PA[j] * TILE_BYTES + ks * 32);
                             const uint64_t bd = tc::smem_desc_sw128(sb + PB[j] * C::B_ROWS_BYTES + ks * 32);
-                            tc::mma_bf16(dst, ad, bd, IDESC, accum);
+                            if constexpr (PAIR) tc::mma_bf16_pair(dst, ad, bd, IDESC, accum);
+                            else tc::mma_bf16(dst, ad, bd, IDESC, accum);
                             accum = 1;
                         }
                     }
-                    tc::mma_commit(&empty[s]);
-                    tc::mma_commit(&accf[b]);
+                    if constexpr (PAIR) {
+                        tc::mma_commit_pair(&empty[s]);
+                        if (last) tc::mma_commit_pair(&accf[b]);
+                    } else {
+                        tc::mma_commit(&empty[s]);
+                        if (last) tc::mma_commit(&accf[b]);
+                    }
+                    if (last) ++ga;
                     any = true;
                 }
             }
-            if (any) tc::mma_commit(doneb);
-            else tc::mbar_expect_tx(doneb, 0);  // nothing issued: complete the barrier's phase now
+            if (any) {
+                if constexpr (PAIR) tc::mma_commit_pair(doneb);
+                else tc::mma_commit(doneb);
+            } else {
+                tc::mbar_expect_tx(doneb, 0);  // nothing issued: complete the barrier's phase now
+                if constexpr (PAIR) tc::mbar_arrive_remote(tc::peer_smem(doneb, 1));
+            }
+        } else if (lane == 0 && PAIR) {
+            // ---------------- relay (odd CTA of a pair) ----------------
+            uint32_t g = 0;
+            for (int u = unit0; u < la.nunits && !*abort_word; u += ustride) {
+                const int ktiles = unit_ktiles(la.tasks[la.units[u].task]);
+                for (int i = 0; i < ktiles; ++i, ++g) {
+                    const int s = g % C::STAGES;
+                    const uint32_t round = g / C::STAGES;
+                    if (!tc::mbar_wait(&full[s], round & 1, abort_word, la.wait_cycles)) {
+                        raise_abort();
+                        break;
+                    }
+                    tc::mbar_arrive_remote(tc::peer_smem(&pfull[s], 0));
+                }
+            }
         }
     } else {
         // ---------------- epilogue warps ----------------
         const int quarter = warp & 3, half = warp >> 2;
         const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
+        const uint32_t acce0 = PAIR ? tc::peer_smem(&acce[0], 0) : tc::smem_u32(&acce[0]);
         uint32_t g = 0;
-        for (int u = blockIdx.x; u < la.nunits; u += gridDim.x) {
+        for (int u = unit0; u < la.nunits; u += ustride) {
             const TcUnit un = la.units[u];
             const TcTask t = la.tasks[un.task];
-            int ktiles = 0;
-            for (int q = 0; q < t.nitem; ++q) ktiles += la.items[t.item0 + q].KT;
+            const int fills = (unit_ktiles(t) + la.kchain - 1) / la.kchain;
             float acc[C::COLS];
 #pragma unroll
             for (int e = 0; e < C::COLS; ++e) acc[e] = 0.f;
             bool ok = !*abort_word;
-            for (int i = 0; i < ktiles && ok; ++i, ++g) {
-                const int b = g & 1;
-                const uint32_t use = g >> 1;
-                if (!tc::mbar_wait(&accf[b], use & 1, abort_word, la.wait_cycles)) {
-                    *abort_word = 1;
+            for (int i = 0; i < fills && ok; ++i, ++g) {
+                const int b = g % C::NACC;
+                const uint32_t use = g / C::NACC;
+                if (!wait_x(&accf[b], use & 1, abort_word)) {
+                    raise_abort();
                     ok = false;
                     break;
                 }
                 tc::fence_after_sync();
+                // 64 columns per load where the registers allow (one wait per 64 columns keeps
+                // the drain short); 128-column halves keep 32 to stay clear of spills
+                constexpr int LB = C::COLS == 64 ? 64 : 32;
 #pragma unroll
-                for (int c0 = 0; c0 < C::COLS; c0 += 32) {
-                    float v[32];
-                    tc::tmem_ld32(tmem + lane_base + (uint32_t)(b * BN + half * C::COLS + c0), v);
+                for (int c0 = 0; c0 < C::COLS; c0 += LB) {
+                    float v[LB];
+                    const uint32_t ta = tmem + lane_base + (uint32_t)(b * BN + half * C::COLS + c0);
+                    if constexpr (LB == 64) tc::tmem_ld64(ta, v);
+                    else tc::tmem_ld32(ta, v);
 #pragma unroll
-                    for (int e = 0; e < 32; ++e) acc[c0 + e] += v[e];
+                    for (int e = 0; e < LB; ++e) acc[c0 + e] += v[e];
                 }
                 tc::fence_before_sync();
                 __syncwarp();
-                if (lane == 0)
-                    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(tc::smem_u32(&acce[b])) : "memory");
+                if (lane == 0) {
+                    if constexpr (PAIR) tc::mbar_arrive_remote(acce0 + (uint32_t)(b * 8));
+                    else asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(acce0 + (uint32_t)(b * 8))
+                                      : "memory");
+                }
             }
             if (!ok || *abort_word) break;
             const PlanArgs *pa = la.plans + t.plan;
             const int nrhs = pa->nrhs;
-            const int r = t.m0 + quarter * 32 + lane;
+            const int r = t.m0 + (int)rank * 128 + quarter * 32 + lane;
             const int beta = t.beta == 2 ? pa->beta_arg : t.beta;
             const int col0 = un.col * BN + half * C::COLS;
             // accumulating outputs: all old values of a 16-column chunk are loaded before any
@@ -489,7 +572,7 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_>::THREADS, 1) tc_gemm_ker
                     }
                 }
                 const int KTv = (t.M + 63) / 64;
-                const int k0 = t.m0 + quarter * 32 + (lane & ~7);
+                const int k0 = t.m0 + (int)rank * 128 + quarter * 32 + (lane & ~7);
                 const bool k_ok = k0 < KTv * 64;
                 const int kt = k0 >> 6;
                 const uint32_t kin = (uint32_t)(k0 & 63);
@@ -519,13 +602,17 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_>::THREADS, 1) tc_gemm_ker
     // all MMAs must be complete before TMEM is released (bounded, also after an abort)
     if (threadIdx.x == 0) {
         volatile int never = 0;
-        if (!tc::mbar_wait(doneb, 0, &never, la.wait_cycles)) *abort_word = 1;
+        if (!wait_x(doneb, 0, &never)) *abort_word = 1;
     }
     __syncthreads();
+    if constexpr (PAIR) tc::cluster_sync();  // no traffic between the two CTAs after this point
     if (*abort_word && threadIdx.x == 0) atomicExch(la.err, MXB_ERR_TIMEOUT);
     tc::fence_before_sync();
     __syncthreads();
-    if (warp == 0) tc::tmem_dealloc(tmem, C::TMEM_COLS);
+    if (warp == 0) {
+        if constexpr (PAIR) tc::tmem_dealloc_pair(tmem, C::TMEM_COLS);
+        else tc::tmem_dealloc(tmem, C::TMEM_COLS);
+    }
 }
 
 int g_sm_count[128];
@@ -539,7 +626,7 @@ int sm_count()
     return g_sm_count[dev];
 }
 
-template <int P, int BN, int S>
+template <int P, int BN, int S, bool PAIR>
 cudaError_t configure_tc()
 {
     static bool done[128];
@@ -548,46 +635,78 @@ cudaError_t configure_tc()
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 128) return cudaErrorInvalidDevice;
     if (done[dev]) return cudaSuccess;
-    e = cudaFuncSetAttribute(tc_gemm_kernel<P, BN, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             TcCfg<P, BN, S>::SMEM);
+    e = cudaFuncSetAttribute(tc_gemm_kernel<P, BN, S, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             TcCfg<P, BN, S, PAIR>::SMEM);
     if (e == cudaSuccess) done[dev] = true;
     return e;
 }
 
-template <int P, int BN, int S>
+template <int P, int BN, int S, bool PAIR>
 cudaError_t launch_tc_cfg(const LaunchArgs &a, cudaStream_t s)
 {
+    using C = TcCfg<P, BN, S, PAIR>;
     if (a.nunits <= 0) return cudaSuccess;
-    cudaError_t e = configure_tc<P, BN, S>();
+    cudaError_t e = configure_tc<P, BN, S, PAIR>();
     if (e != cudaSuccess) return e;
-    const int grid = std::min(a.nunits, sm_count());
-    tc_gemm_kernel<P, BN, S><<<grid, TcCfg<P, BN, S>::THREADS, TcCfg<P, BN, S>::SMEM, s>>>(a);
-    return cudaGetLastError();
+    if constexpr (!PAIR) {
+        const int grid = std::min(a.nunits, sm_count());
+        tc_gemm_kernel<P, BN, S, false><<<grid, C::THREADS, C::SMEM, s>>>(a);
+        return cudaGetLastError();
+    } else {
+        const int pairs = std::min(a.nunits, std::max(1, sm_count() / 2));
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)(2 * pairs), 1, 1);
+        cfg.blockDim = dim3(C::THREADS, 1, 1);
+        cfg.dynamicSmemBytes = C::SMEM;
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = 2;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        return cudaLaunchKernelEx(&cfg, tc_gemm_kernel<P, BN, S, true>, a);
+    }
 }
 
 // Column-tile widths per product count; pipeline depth fills ~192-216 KiB of shared memory.
-cudaError_t launch_tc(int P, int BN, const LaunchArgs &a, cudaStream_t s)
+// A pair stages half of B per CTA, which buys a deeper pipeline at the same width.
+cudaError_t launch_tc(int P, int BN, bool pair, const LaunchArgs &a, cudaStream_t s)
 {
-    if (P == 2) {
-        if (BN == 256) return launch_tc_cfg<2, 256, 2>(a, s);
-        if (BN == 128) return launch_tc_cfg<2, 128, 3>(a, s);
-        return launch_tc_cfg<2, 64, 4>(a, s);
+    if (pair) {
+        if (P == 2) return BN == 256 ? launch_tc_cfg<2, 256, 3, true>(a, s) : launch_tc_cfg<2, 128, 4, true>(a, s);
+        return BN == 256 ? launch_tc_cfg<3, 256, 2, true>(a, s) : launch_tc_cfg<3, 128, 3, true>(a, s);
     }
-    if (BN == 128) return launch_tc_cfg<3, 128, 2>(a, s);
-    return launch_tc_cfg<3, 64, 3>(a, s);
+    if (P == 2) {
+        if (BN == 256) return launch_tc_cfg<2, 256, 2, false>(a, s);
+        if (BN == 128) return launch_tc_cfg<2, 128, 3, false>(a, s);
+        return launch_tc_cfg<2, 64, 4, false>(a, s);
+    }
+    if (BN == 128) return launch_tc_cfg<3, 128, 2, false>(a, s);
+    return launch_tc_cfg<3, 64, 3, false>(a, s);
 }
 
 cudaError_t configure_all_tc()
 {
-    cudaError_t e = configure_tc<2, 256, 2>();
-    if (e == cudaSuccess) e = configure_tc<2, 128, 3>();
-    if (e == cudaSuccess) e = configure_tc<2, 64, 4>();
-    if (e == cudaSuccess) e = configure_tc<3, 128, 2>();
-    if (e == cudaSuccess) e = configure_tc<3, 64, 3>();
+    cudaError_t e = configure_tc<2, 256, 2, false>();
+    if (e == cudaSuccess) e = configure_tc<2, 128, 3, false>();
+    if (e == cudaSuccess) e = configure_tc<2, 64, 4, false>();
+    if (e == cudaSuccess) e = configure_tc<3, 128, 2, false>();
+    if (e == cudaSuccess) e = configure_tc<3, 64, 3, false>();
+    if (e == cudaSuccess) e = configure_tc<2, 256, 3, true>();
+    if (e == cudaSuccess) e = configure_tc<2, 128, 4, true>();
+    if (e == cudaSuccess) e = configure_tc<3, 256, 2, true>();
+    if (e == cudaSuccess) e = configure_tc<3, 128, 3, true>();
     return e;
 }
 
 int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// Tile code of a tensor-core launch: column-tile width, plus MXB_TILE_PAIR when the launch
+// runs on CTA pairs (256-row tiles).
+int tile_width(int code) { return code & (MXB_TILE_PAIR - 1); }
+bool tile_pair(int code) { return (code & MXB_TILE_PAIR) != 0; }
 
 // Position of an op in the evaluation sequence; ops of different plans with the same key run
 // in one launch.  W split, up-sweep by height, then for every depth far followed by down,
@@ -647,6 +766,7 @@ struct Batch : public mxb_batch {
         int phase, level, P, a_pool, b_buf, t_buf;
         int first, count;  // range in the merged tasks or jobs
         int max_kt;
+        int max_m;         // tallest output block (pairs only pay off above 128 rows)
     };
     std::vector<MOp> ops;
     std::vector<TcTask> tasks;
@@ -732,6 +852,7 @@ int Batch::build(const std::vector<Plan *> &ps)
         m.b_buf = o0->b_buf;
         m.t_buf = o0->t_buf;
         m.max_kt = 1;
+        m.max_m = 0;
         if (m.phase == PH_SPLITW) {
             m.first = (int)jobs.size();
             for (auto &po : kv.second) {
@@ -755,6 +876,7 @@ int Batch::build(const std::vector<Plan *> &ps)
                     for (int q = 0; q < t.nitem; ++q) items.push_back(S.items[t.item0 + q]);
                     t.item0 = item0;
                     t.plan = po.first;
+                    m.max_m = std::max(m.max_m, t.M);
                     tasks.push_back(t);
                 }
             }
@@ -794,8 +916,10 @@ int Batch::units_for(Entry &e, const std::vector<int> &bn)
         const MOp &m = ops[k];
         e.unit_first[k] = (int)units.size();
         if (m.phase == PH_SPLITW) continue;
+        const bool pair = tile_pair(bn[k]);
         for (int t = m.first; t < m.first + m.count; ++t) {
-            const int ncol = (int)ceil_div(e.nrhs[tasks[t].plan], bn[k]);
+            if (pair && tasks[t].m0 % 256) continue;  // the pair's odd CTA takes rows m0 + 128
+            const int ncol = (int)ceil_div(e.nrhs[tasks[t].plan], tile_width(bn[k]));
             for (int c = 0; c < ncol; ++c) units.push_back(TcUnit{t, c});
         }
         e.unit_count[k] = (int)units.size() - e.unit_first[k];
@@ -807,6 +931,10 @@ int Batch::units_for(Entry &e, const std::vector<int> &bn)
         err = cudaMemcpy(e.dUnits, units.data(), units.size() * sizeof(TcUnit), cudaMemcpyHostToDevice);
     if (err != cudaSuccess) return batch_fail(std::string("work units: ") + cudaGetErrorString(err), MXB_ERR_CUDA);
     return MXB_OK;
+}
+
+namespace {
+int kchain_for(int P);
 }
 
 int Batch::enqueue(Entry &e, cudaStream_t stream, int debug_flags, long long wait_cycles, const std::vector<int> &bn,
@@ -838,7 +966,8 @@ int Batch::enqueue(Entry &e, cudaStream_t stream, int debug_flags, long long wai
                 a.err = plans[0]->bf16->dErr;
                 a.wait_cycles = wait_cycles > 0 ? wait_cycles : tc::WAIT_CYCLES;
                 a.stall_test = (debug_flags & MXB_DEBUG_STALL_ONE_WAIT) && first_tc;
-                err = launch_tc(m.P, bn[k], a, stream);
+                a.kchain = kchain_for(m.P);
+                err = launch_tc(m.P, tile_width(bn[k]), tile_pair(bn[k]), a, stream);
             }
             first_tc = false;
         }
@@ -880,6 +1009,41 @@ int default_bn(int P, int nrhs_max)
 {
     if (P == 2) return nrhs_max > 128 ? 256 : (nrhs_max > 64 ? 128 : 64);
     return nrhs_max > 64 ? 128 : 64;
+}
+
+// MXB_TC_TILE=<code> runs every tensor-core launch with that tile (width, + MXB_TILE_PAIR for
+// pairs), mapped to the nearest variant the launch's product count has; read when an
+// evaluation graph is built.  For tests that must reach one kernel variant.
+int forced_tile(int P)
+{
+    const char *e = getenv("MXB_TC_TILE");
+    const int code = e && *e ? atoi(e) : 0;
+    if (code <= 0) return 0;
+    const int w = tile_width(code);
+    if (tile_pair(code)) return (w >= 256 ? 256 : 128) | MXB_TILE_PAIR;
+    if (P == 2) return w >= 256 ? 256 : (w >= 128 ? 128 : 64);
+    return w >= 128 ? 128 : 64;
+}
+
+// K tiles per accumulator fill: 2 for bf16x3 products, 1 for bf16x6 (MXB_TC_KCHAIN overrides).
+int kchain_for(int P)
+{
+    static const int forced = [] {
+        const char *e = getenv("MXB_TC_KCHAIN");
+        const int k = e && *e ? atoi(e) : 0;
+        return k == 1 || k == 2 ? k : 0;
+    }();
+    return forced ? forced : (P == 2 ? 2 : 1);
+}
+
+// MXB_TC_PAIRS=0 keeps the autotuner to single-CTA launches.
+bool pairs_enabled()
+{
+    static const bool on = [] {
+        const char *e = getenv("MXB_TC_PAIRS");
+        return !(e && *e == '0');
+    }();
+    return on;
 }
 
 bool autotune_enabled()
@@ -929,23 +1093,36 @@ int Batch::tune(Entry &e, std::vector<PlanArgs> pa, std::vector<int> &bn, cudaSt
             if (!rc) rc = enqueue(te, stream, 0, wait_cycles, bn, (int)k);
             continue;
         }
-        const std::vector<int> cands = ops[k].P == 2 ? std::vector<int>{256, 128, 64} : std::vector<int>{128, 64};
+        std::vector<int> cands = ops[k].P == 2 ? std::vector<int>{256, 128, 64} : std::vector<int>{128, 64};
+        if (ops[k].max_m > 128 && pairs_enabled()) {
+            cands.push_back(256 | MXB_TILE_PAIR);
+            cands.push_back(128 | MXB_TILE_PAIR);
+        }
         float best = 1e30f;
         int best_bn = bn[k];
         for (int c : cands) {
-            if (c > 2 * std::max(64, maxn)) continue;
+            if (tile_width(c) > 2 * std::max(64, maxn)) continue;
             std::vector<int> trial = bn;
             trial[k] = c;
             rc = units_for(te, trial);
             float ms = 0.f;
-            for (int rep = 0; rep < 2 && !rc; ++rep) {
+            bool refused = false;
+            for (int rep = 0; rep < 2 && !rc && !refused; ++rep) {
                 cudaEventRecord(e0, stream);
-                rc = enqueue(te, stream, 0, wait_cycles, trial, (int)k);
+                const int lrc = enqueue(te, stream, 0, wait_cycles, trial, (int)k);
                 cudaEventRecord(e1, stream);
-                if (!rc && cudaEventSynchronize(e1) != cudaSuccess) rc = batch_fail("autotune sync", MXB_ERR_CUDA);
+                if (lrc) {
+                    // a launch the device refuses (e.g. no room for a cluster) is not a candidate;
+                    // launch-configuration errors are not sticky
+                    refused = true;
+                    (void)cudaGetLastError();
+                    continue;
+                }
+                if (cudaEventSynchronize(e1) != cudaSuccess) rc = batch_fail("autotune sync", MXB_ERR_CUDA);
                 if (!rc) cudaEventElapsedTime(&ms, e0, e1);
             }
             if (rc) break;
+            if (refused) continue;
             if (ms < best) {
                 best = ms;
                 best_bn = c;
@@ -1024,7 +1201,10 @@ int Batch::evaluate(const double *const *W, double *const *Y, const int *nrhs, i
         for (size_t k = 0; k < ops.size(); ++k)
             if (ops[k].phase != PH_SPLITW) bn[k] = default_bn(ops[k].P, maxn);
         auto t = tuned.find(nr);
-        if (t != tuned.end()) {
+        if (forced_tile(2)) {
+            for (size_t k = 0; k < ops.size(); ++k)
+                if (ops[k].phase != PH_SPLITW) bn[k] = forced_tile(ops[k].P);
+        } else if (t != tuned.end()) {
             bn = t->second;
         } else if (autotune_enabled() && !debug_flags) {
             int rc = tune(e, pa, bn, stream, wait_cycles);
@@ -1117,16 +1297,18 @@ int Batch::profile(const double *const *W, double *const *Y, const int *nrhs, cu
         o = mxb_op_profile{};
         o.phase = m.phase;
         o.level = m.level;
-        o.width = e->bn[k];
+        o.width = tile_width(e->bn[k]);
+        o.pair = tile_pair(e->bn[k]) ? 1 : 0;
         o.units = e->unit_count[k];
         const double products = m.P == 2 ? 3.0 : 6.0;
+        const int tile_rows = o.pair ? 256 : 128;
         for (int u = e->unit_first[k]; u < e->unit_first[k] + e->unit_count[k]; ++u) {
             const TcTask &t = tasks[units[u].task];
-            const double rows = std::min(128, t.M - t.m0);
+            const double rows = std::min(tile_rows, t.M - t.m0);
             const double cols = std::min(o.width, nr[t.plan] - units[u].col * o.width);
             for (int q = t.item0; q < t.item0 + t.nitem; ++q) {
                 o.flops += 2.0 * rows * items[q].K * cols;
-                o.issued_flops += products * 2.0 * 128 * (64.0 * items[q].KT) * o.width;
+                o.issued_flops += products * 2.0 * tile_rows * (64.0 * items[q].KT) * o.width;
             }
         }
         cudaEventElapsedTime(&o.ms, ev[k], ev[k + 1]);

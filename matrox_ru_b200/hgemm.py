@@ -194,7 +194,7 @@ def cds_desc(cds, keep: list) -> _lib.CdsDesc:
 
 def _profile_records(recs, n):
     return [{"phase": _lib.PHASES.get(r.phase, str(r.phase)), "level": r.level, "width": r.width, "units": r.units,
-             "flops": r.flops, "issued_flops": r.issued_flops, "ms": r.ms} for r in recs[:min(n, len(recs))]]
+             "pair": bool(r.pair), "flops": r.flops, "issued_flops": r.issued_flops, "ms": r.ms} for r in recs[:min(n, len(recs))]]
 
 
 class Plan:
@@ -353,7 +353,9 @@ class Batch:
         l, nw = I32(), I32()
         widths = (I32 * 256)()
         check(_lib.load().mxb_batch_info(self._h, ctypes.byref(l), widths, 256, ctypes.byref(nw)), "mxb_batch_info")
-        return {"launches": int(l.value), "widths": [int(widths[i]) for i in range(nw.value)]}
+        codes = [int(widths[i]) for i in range(nw.value)]
+        return {"launches": int(l.value), "widths": [c & (_lib.TILE_PAIR - 1) for c in codes],
+                "pairs": [bool(c & _lib.TILE_PAIR) for c in codes]}
 
 
 class Evaluator:
