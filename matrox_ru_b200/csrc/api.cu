@@ -47,11 +47,15 @@ struct CacheEntry {
 std::list<CacheEntry> g_cache;  // most recent first
 constexpr size_t kCacheSlots = 4;
 
+// Per-device state of the drop-ins.  An evaluation runs over column slabs of the right-hand
+// sides: slab k's upload (stream `in`), evaluation (`stream`) and download (`out`) overlap with
+// the neighbouring slabs', with two W and two Y slab buffers in rotation.
 struct DeviceBuffers {
     int device = -1;
-    cudaStream_t stream = nullptr;
-    double *W = nullptr, *Y = nullptr;
-    size_t wcap = 0, ycap = 0;
+    cudaStream_t stream = nullptr, in = nullptr, out = nullptr;
+    double *W[2] = {nullptr, nullptr}, *Y[2] = {nullptr, nullptr};
+    size_t wcap[2] = {0, 0}, ycap[2] = {0, 0};
+    cudaEvent_t uploaded[2] = {}, computed[2] = {}, downloaded[2] = {};
 };
 DeviceBuffers g_buf[64];
 
@@ -130,10 +134,77 @@ DeviceBuffers *buffers()
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
     DeviceBuffers &b = g_buf[dev];
     if (!b.stream) {
-        if (cudaStreamCreateWithFlags(&b.stream, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+        cudaStream_t s[3] = {};
+        cudaEvent_t e[6] = {};
+        bool ok = true;
+        for (cudaStream_t &x : s) ok = ok && cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking) == cudaSuccess;
+        for (cudaEvent_t &x : e) ok = ok && cudaEventCreateWithFlags(&x, cudaEventDisableTiming) == cudaSuccess;
+        if (!ok) {
+            for (cudaStream_t x : s)
+                if (x) cudaStreamDestroy(x);
+            for (cudaEvent_t x : e)
+                if (x) cudaEventDestroy(x);
+            return nullptr;
+        }
+        b.in = s[1];
+        b.out = s[2];
+        for (int i = 0; i < 2; ++i) {
+            b.uploaded[i] = e[i];
+            b.computed[i] = e[2 + i];
+            b.downloaded[i] = e[4 + i];
+        }
         b.device = dev;
+        b.stream = s[0];
     }
     return &b;
+}
+
+// Columns per slab of a drop-in evaluation: about eight slabs, at least 128 columns each
+// (narrower slabs lose tensor-core efficiency), a multiple of 64.  MXB_DROPIN_SLAB=<columns>
+// overrides it; MXB_DROPIN_SLAB=0 evaluates all columns as one slab.
+int slab_columns(int nrhs)
+{
+    static const int forced = [] {
+        const char *e = getenv("MXB_DROPIN_SLAB");
+        return e && *e ? atoi(e) : -1;
+    }();
+    if (forced == 0) return nrhs;
+    if (forced > 0) return std::min(forced, nrhs);
+    const int c = ((nrhs + 7) / 8 + 63) / 64 * 64;
+    return std::min(nrhs, std::max(128, c));
+}
+
+// Copies columns [j0, j0 + cw) of every leaf block between the caller's host array (leaf i's
+// block, Ddim[i] x nrhs column-major, at element offset hofs[i]) and a packed device slab
+// (leaf i's block, Ddim[i] x cw, at leaf_row[i] * cw).  Runs of leaves with equal sizes and
+// evenly spaced host blocks move as one 2-D copy.
+cudaError_t copy_slab(const Plan &p, double *host, const int32_t *hofs, double *dev, int j0, int cw, bool to_device,
+                      cudaStream_t s)
+{
+    const int n = p.nleaf;
+    for (int i = 0; i < n;) {
+        const int m = p.Ddim[i];
+        int g = 1;
+        const int64_t stride = i + 1 < n ? (int64_t)hofs[i + 1] - hofs[i] : 0;
+        if (m > 0 && stride >= (int64_t)m * cw && stride * (int64_t)sizeof(double) < (int64_t)INT32_MAX)
+            while (i + g < n && p.Ddim[i + g] == m && (int64_t)hofs[i + g] - hofs[i + g - 1] == stride) ++g;
+        if (m > 0) {
+            double *h = host + hofs[i] + (size_t)j0 * m;
+            double *d = dev + (size_t)p.leaf_row[i] * cw;
+            const size_t width = (size_t)m * cw * sizeof(double);
+            cudaError_t e;
+            if (g == 1)
+                e = cudaMemcpyAsync(to_device ? (void *)d : (void *)h, to_device ? (const void *)h : (const void *)d,
+                                    width, to_device ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost, s);
+            else if (to_device)
+                e = cudaMemcpy2DAsync(d, width, h, (size_t)stride * sizeof(double), width, g, cudaMemcpyHostToDevice, s);
+            else
+                e = cudaMemcpy2DAsync(h, (size_t)stride * sizeof(double), d, width, width, g, cudaMemcpyDeviceToHost, s);
+            if (e != cudaSuccess) return e;
+        }
+        i += g;
+    }
+    return cudaSuccess;
 }
 
 int grow(double **p, size_t *cap, size_t elems)
@@ -284,32 +355,55 @@ int run_dropin(DropIn &a)
         set_error("cannot create the drop-in stream");
         return MXB_ERR_CUDA;
     }
-    // extents of the caller's leaf-blocked W and Y
-    size_t wext = 0, yext = 0;
     for (int i = 0; i < a.nleaf; ++i) {
         if (a.wptr[i] < 0 || a.uptr[i] < 0) {
             set_error("negative leaf offset");
             return MXB_ERR_STRUCTURE;
         }
-        wext = std::max<size_t>(wext, (size_t)a.wptr[i] + (size_t)a.Ddim[i] * a.nrhs);
-        yext = std::max<size_t>(yext, (size_t)a.uptr[i] + (size_t)a.Ddim[i] * a.nrhs);
     }
-    rc = grow(&buf->W, &buf->wcap, wext);
-    if (rc) return rc;
-    rc = grow(&buf->Y, &buf->ycap, yext);
-    if (rc) return rc;
-    cudaStream_t s = buf->stream;
-    API_CUDA(cudaMemcpyAsync(buf->W, a.mrhs, wext * sizeof(double), cudaMemcpyHostToDevice, s));
-    const bool accumulate = !a.hss;
-    if (accumulate && !(g_flags & MXB_FLAG_OUTPUT_IS_ZERO))
-        API_CUDA(cudaMemcpyAsync(buf->Y, a.apres, yext * sizeof(double), cudaMemcpyHostToDevice, s));
-    else if (accumulate)
-        API_CUDA(cudaMemsetAsync(buf->Y, 0, yext * sizeof(double), s));
-    rc = plan->run(plan->launches_fwd, buf->W, buf->Y, a.nrhs, a.wptr, a.uptr, accumulate ? 1 : 0, s);
-    if (rc) return rc;
-    API_CUDA(cudaMemcpyAsync(a.apres, buf->Y, yext * sizeof(double), cudaMemcpyDeviceToHost, s));
-    API_CUDA(cudaStreamSynchronize(s));
-    if ((g_flags & MXB_FLAG_MIRROR_WORKSPACES) && plan->precision == MXB_PREC_FP64) {
+    const bool mirror = (g_flags & MXB_FLAG_MIRROR_WORKSPACES) && plan->precision == MXB_PREC_FP64;
+    // Column slabs: the skeleton workspaces of one evaluation cover only its own columns, so
+    // mirroring them back needs all columns in one slab.
+    const int cw = mirror ? a.nrhs : slab_columns(a.nrhs);
+    const int nslab = (a.nrhs + cw - 1) / cw;
+    const size_t slab_elems = (size_t)std::max<int64_t>(plan->rows_total, 1) * cw;
+    for (int b = 0; b < std::min(nslab, 2); ++b) {
+        rc = grow(&buf->W[b], &buf->wcap[b], slab_elems);
+        if (rc) return rc;
+        rc = grow(&buf->Y[b], &buf->ycap[b], slab_elems);
+        if (rc) return rc;
+    }
+    // H2-b accumulates into apres (near beta = 1), HSS overwrites it
+    const bool upload_y = !a.hss && !(g_flags & MXB_FLAG_OUTPUT_IS_ZERO);
+    // slab k uses buffers k % 2.  Upload k waits until evaluation k-2 has read W[b] (and, for
+    // an uploaded Y, until download k-2 has read Y[b]); evaluation k waits for upload k and for
+    // download k-2; download k waits for evaluation k.
+    for (int k = 0; k < nslab; ++k) {
+        const int b = k & 1, j0 = k * cw, w = std::min(cw, a.nrhs - j0);
+        if (k >= 2) {
+            API_CUDA(cudaStreamWaitEvent(buf->in, buf->computed[b], 0));
+            if (upload_y) API_CUDA(cudaStreamWaitEvent(buf->in, buf->downloaded[b], 0));
+        }
+        API_CUDA(copy_slab(*plan, a.mrhs, a.wptr, buf->W[b], j0, w, true, buf->in));
+        if (upload_y) API_CUDA(copy_slab(*plan, a.apres, a.uptr, buf->Y[b], j0, w, true, buf->in));
+        API_CUDA(cudaEventRecord(buf->uploaded[b], buf->in));
+        API_CUDA(cudaStreamWaitEvent(buf->stream, buf->uploaded[b], 0));
+        if (k >= 2) API_CUDA(cudaStreamWaitEvent(buf->stream, buf->downloaded[b], 0));
+        // a Y known to be zero is overwritten instead of accumulated into
+        rc = plan->run(plan->launches_fwd, buf->W[b], buf->Y[b], w, nullptr, nullptr, upload_y ? 1 : 0,
+                       buf->stream);
+        if (rc) {
+            cudaDeviceSynchronize();
+            return rc;
+        }
+        API_CUDA(cudaEventRecord(buf->computed[b], buf->stream));
+        API_CUDA(cudaStreamWaitEvent(buf->out, buf->computed[b], 0));
+        API_CUDA(copy_slab(*plan, a.apres, a.uptr, buf->Y[b], j0, w, false, buf->out));
+        API_CUDA(cudaEventRecord(buf->downloaded[b], buf->out));
+    }
+    API_CUDA(cudaStreamSynchronize(buf->out));
+    API_CUDA(cudaStreamSynchronize(buf->stream));
+    if (mirror) {
         rc = plan->read_workspaces(a.nrhs, a.wsko, a.wskel, a.usko, a.uskel);
         if (rc) return rc;
     }
