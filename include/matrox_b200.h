@@ -267,12 +267,14 @@ MXB_API int32_t mxb_batch_destroy(mxb_batch *batch);
  * is the ordinary result.  The call synchronises `stream`. */
 #define MXB_PHASE_SPLIT_W 0        /* W -> bf16 operand tiles (split-BF16 plans) */
 #define MXB_PHASE_UP 1             /* leaf projection (level 0) or transfer at height `level` */
-#define MXB_PHASE_FAR 2            /* far couplings into the nodes at depth `level` */
+#define MXB_PHASE_FAR 2            /* far couplings of every depth (one launch) */
 #define MXB_PHASE_DOWN 3           /* downward transfer into the nodes at depth `level` */
 #define MXB_PHASE_NEAR 4           /* near field */
 #define MXB_PHASE_LEAF_DOWN 5      /* leaf downward projection into Y */
 #define MXB_PHASE_FAR_DOWN 6       /* FP64 plans: far + downward transfer, depth `level` */
 #define MXB_PHASE_NEAR_LEAF_DOWN 7 /* FP64 plans: near field + leaf downward projection */
+#define MXB_PHASE_FAR_NEAR 8       /* far couplings of every depth and the near field, one launch
+                                      (split plans whose near and far products agree)    */
 typedef struct mxb_op_profile {
     int32_t phase;        /* MXB_PHASE_* */
     int32_t level;        /* height or depth, see the phase */

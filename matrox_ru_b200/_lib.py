@@ -28,7 +28,7 @@ FLAG_OUTPUT_IS_ZERO = 2
 DEBUG_STALL_ONE_WAIT = 1
 TILE_PAIR = 4096
 PHASES = {0: "split_w", 1: "up", 2: "far", 3: "down", 4: "near", 5: "leaf_down", 6: "far_down",
-          7: "near_leaf_down"}
+          7: "near_leaf_down", 8: "far_near"}
 
 P = ctypes.c_void_p
 I32 = ctypes.c_int32

@@ -61,11 +61,15 @@ enum APool { POOL_NEAR, POOL_FAR, POOL_VU3, POOL_VD3, NPOOL };
 enum BBuf { BUF_W, BUF_WSKEL, BUF_USKEL, NBUF };
 
 struct TcItem {
-    uint64_t a_off;   // byte offset of A's tile (0, 0) in the plan's A pool of the launch
-    int64_t b_base;   // K-tile base of the B operand's node / leaf in the B buffer
+    uint64_t a_off;   // byte offset of A's tile (0, 0) in the plan's A pool `a_pool`
+    int64_t b_base;   // K-tile base of the B operand's node / leaf in the B buffer `b_buf`
     int32_t KT;       // K tiles of this item
     int32_t K;        // K before padding to whole tiles (flop accounting)
+    int16_t a_pool;   // APool of A
+    int16_t b_buf;    // BBuf of B
+    int32_t pad;
 };
+static_assert(sizeof(TcItem) == 32, "TcItem layout");
 
 // Output of a tensor-core task.
 enum OutKind : int16_t {
@@ -85,7 +89,7 @@ struct TcTask {
     int32_t plan;    // index into the launch's plan table
     int16_t out_kind;
     int16_t beta;    // 0 overwrite, 1 accumulate (OUT_TILES: add the FP32 block), 2 plan's arg
-    int32_t pad;
+    int32_t t_buf;   // BBuf that OUT_TILES writes
 };
 
 struct TcUnit {
@@ -125,10 +129,10 @@ struct LaunchArgs {
     const TcTask *tasks;
     const TcItem *items;
     const TcUnit *units;
+    int *next_unit;         // work-unit counter of this launch, zero at launch
     int *err;
     long long wait_cycles;  // limit of every wait in the kernel
     int nunits;
-    int a_pool, b_buf, t_buf;
     int stall_test;         // test hook: CTA 0 withholds its first stage, so a wait runs out
     int kchain;             // K tiles accumulated per TMEM accumulator fill (1 or 2)
 };
@@ -239,9 +243,13 @@ struct TcCfg {
     static constexpr int A_BYTES = P * TILE_BYTES;
     static constexpr int B_BYTES = P * B_ROWS_BYTES;
     static constexpr int STAGE = A_BYTES + B_BYTES;
-    static constexpr int SMEM = STAGES * STAGE + 1024 + 256;
+    static constexpr int SMEM = STAGES * STAGE + 1024 + 1024;  // + alignment, barriers, unit ring
     static constexpr int NPROD = P == 2 ? 3 : 6;
     static constexpr int EPI_WARPS = 8;          // two per TMEM lane quarter, one per column half
+    static constexpr int RING = 16;              // work units published ahead of the readers
+    // readers of a ring slot: MMA issuer and epilogue warps (+ the odd CTA's producer, relay
+    // and epilogue warps in a pair)
+    static constexpr int RING_READERS = PAIR ? 2 * (1 + EPI_WARPS) + 1 : 1 + EPI_WARPS;
     static constexpr int THREADS = (EPI_WARPS + 2) * 32;
     static constexpr int COLS = BN / 2;          // accumulator columns per epilogue thread
     static constexpr int NACC = BN >= 256 ? 2 : 4;  // TMEM accumulator buffers (512 columns at most)
@@ -258,9 +266,12 @@ struct TcCfg {
 // epilogue warps add every tile's partial sums into per-thread FP32 registers with ordinary
 // round-to-nearest adds while the tensor core already works on the next tiles.
 //
-// Persistent: CTA (or CTA pair) b walks the units b, b + grid, ...  The roles walk the same
-// sequence, so one K-tile counter drives every stage and accumulator phase; TMEM and the
-// barriers are set up once, and the epilogue of one unit overlaps the MMAs of the next.
+// Persistent with dynamic scheduling: the producer thread of a CTA (of the even CTA of a pair)
+// claims work units from the launch's counter in list order (longest first) and publishes each
+// unit in a ring in shared memory (in both CTAs of a pair); every role reads the ring, so all
+// roles walk the same sequence, and one K-tile counter drives every stage and accumulator
+// phase.  TMEM and the barriers are set up once, and the epilogue of one unit overlaps the
+// MMAs of the next.  A unit of -1 ends the sequence.
 //
 // In a pair the even CTA issues the MMAs.  The odd CTA's MMA-warp thread relays "my stage has
 // landed" to the even CTA's pfull barrier, its epilogue warps arrive on the even CTA's acce
@@ -270,6 +281,7 @@ template <int P, int BN, int STAGES_, bool PAIR>
 __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_gemm_kernel(LaunchArgs la)
 {
     using C = TcCfg<P, BN, STAGES_, PAIR>;
+    constexpr int RING = C::RING;
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + C::STAGES * C::STAGE);
@@ -278,14 +290,15 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
     uint64_t *accf = pfull + C::STAGES;   // accumulator buffer b holds a finished K tile
     uint64_t *acce = accf + C::NACC;      // accumulator buffer b has been drained
     uint64_t *doneb = acce + C::NACC;     // every MMA of this CTA (pair) has completed
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(doneb + 1);
+    uint64_t *ufull = doneb + 1;          // ring slot i holds a unit
+    uint64_t *uempty = ufull + RING;      // every reader of ring slot i has taken its unit
+    volatile int *ring = reinterpret_cast<volatile int *>(uempty + RING);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(const_cast<int *>(ring) + RING);
     volatile int *abort_word = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t rank = PAIR ? tc::cluster_ctarank() : 0u;
     const bool issuer = rank == 0;
-    const int unit0 = PAIR ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
-    const int ustride = PAIR ? (int)(gridDim.x >> 1) : (int)gridDim.x;
     auto raise_abort = [&]() {
         *abort_word = 1;
         if constexpr (PAIR) tc::st_remote_u32(tc::peer_smem((const void *)abort_word, rank ^ 1u), 1u);
@@ -294,6 +307,25 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
     auto wait_x = [&](uint64_t *bar, uint32_t parity, volatile int *ab) {
         if constexpr (PAIR) return tc::mbar_wait_cluster(bar, parity, ab, la.wait_cycles);
         else return tc::mbar_wait(bar, parity, ab, la.wait_cycles);
+    };
+    auto arrive_local = [&](uint64_t *bar) {
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(tc::smem_u32(bar)) : "memory");
+    };
+    // Next unit of the ring for a reader (one thread): waits for slot `slot`, takes the unit
+    // and releases the slot to the producer (in the even CTA of a pair).  -2: a wait gave up.
+    auto take_unit = [&](uint32_t &slot) -> int {
+        const int i = (int)(slot % RING);
+        const uint32_t parity = (slot / RING) & 1u;
+        ++slot;
+        int u = -2;
+        if (wait_x(&ufull[i], parity, abort_word)) u = ring[i];
+        if constexpr (PAIR) {
+            if (rank == 1) tc::mbar_arrive_remote(tc::peer_smem(&uempty[i], 0));
+            else arrive_local(&uempty[i]);
+        } else {
+            arrive_local(&uempty[i]);
+        }
+        return u;
     };
 
     if (threadIdx.x == 0) {
@@ -307,6 +339,10 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
             tc::mbar_init(&acce[b], C::EPI_WARPS * (PAIR ? 2 : 1));
         }
         tc::mbar_init(doneb, 1);
+        for (int i = 0; i < RING; ++i) {
+            tc::mbar_init(&ufull[i], 1);
+            tc::mbar_init(&uempty[i], C::RING_READERS);
+        }
         *abort_word = 0;
         tc::fence_mbar_init();
     }
@@ -330,15 +366,41 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
         if (lane == 0) {
             // ---------------- producer ----------------
             uint32_t g = 0;               // K-tile counter of this CTA
+            uint32_t slot = 0;            // ring counter
             uint32_t filled[C::STAGES];   // rounds filled per stage (drained before exit)
 #pragma unroll
             for (int s = 0; s < C::STAGES; ++s) filled[s] = 0;
-            for (int u = unit0; u < la.nunits && !*abort_word; u += ustride) {
+            bool stop = false;
+            while (!stop && !*abort_word) {
+                int u;
+                if (!PAIR || issuer) {
+                    // claim the next unit and publish it to every reader
+                    u = atomicAdd(la.next_unit, 1);
+                    if (u >= la.nunits) u = -1;
+                    const int i = (int)(slot % RING);
+                    const uint32_t round = slot / RING;
+                    ++slot;
+                    if (!wait_x(&uempty[i], (round & 1) ^ 1, abort_word)) {
+                        raise_abort();
+                        break;
+                    }
+                    ring[i] = u;
+                    if constexpr (PAIR) {
+                        tc::st_remote_u32(tc::peer_smem((const void *)&ring[i], 1), (uint32_t)u);
+                        tc::mbar_arrive_remote(tc::peer_smem(&ufull[i], 1));
+                    }
+                    arrive_local(&ufull[i]);
+                } else {
+                    u = take_unit(slot);
+                    if (u == -2) {
+                        raise_abort();
+                        break;
+                    }
+                }
+                if (u < 0) break;
                 const TcUnit un = la.units[u];
                 const TcTask t = la.tasks[un.task];
                 const PlanArgs *pa = la.plans + t.plan;
-                const uint8_t *a_pool = pa->pool[la.a_pool];
-                const uint8_t *b_pool = pa->buf[la.b_buf];
                 const int NT = pa->NT;
                 const int cb = un.col * BN + (int)rank * C::B_ROWS;  // first B row staged here
                 const TcItem *ti = la.items + t.item0;
@@ -347,13 +409,16 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                 // MMA rows it feeds are never stored
                 const bool a_ok = !PAIR || issuer || t.m0 + 128 < t.M;
                 const uint32_t tx = (a_ok ? C::A_BYTES : 0) + C::B_BYTES;
-                for (int q = 0; q < t.nitem && !*abort_word; ++q) {
+                for (int q = 0; q < t.nitem && !stop; ++q) {
                     const TcItem it = ti[q];
+                    const uint8_t *a_pool = pa->pool[it.a_pool];
+                    const uint8_t *b_pool = pa->buf[it.b_buf];
                     for (int kt = 0; kt < it.KT; ++kt, ++g) {
                         const int s = g % C::STAGES;
                         const uint32_t round = g / C::STAGES;
                         if (!wait_x(&empty[s], (round & 1) ^ 1, abort_word)) {
                             raise_abort();
+                            stop = true;
                             break;
                         }
                         if (la.stall_test && blockIdx.x == 0 && g == 0) continue;  // never filled
@@ -405,10 +470,16 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
             constexpr uint32_t IDESC = tc::idesc_bf16_f32(C::M_MMA, BN);
             constexpr int PA[6] = {0, 0, 1, 0, 1, 2};
             constexpr int PB[6] = {0, 1, 0, 2, 1, 0};
-            uint32_t g = 0;   // K-tile (stage) counter
-            uint32_t ga = 0;  // accumulator-fill counter
-            bool any = false;
-            for (int u = unit0; u < la.nunits && !*abort_word; u += ustride) {
+            uint32_t g = 0;     // K-tile (stage) counter
+            uint32_t ga = 0;    // accumulator-fill counter
+            uint32_t slot = 0;  // ring counter
+            bool any = false, stop = false;
+            while (!stop) {
+                const int u = take_unit(slot);
+                if (u < 0) {
+                    if (u == -2) raise_abort();
+                    break;
+                }
                 const int ktiles = unit_ktiles(la.tasks[la.units[u].task]);
                 for (int i = 0; i < ktiles; ++i, ++g) {
                     const int s = g % C::STAGES;
@@ -421,6 +492,7 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                         !tc::mbar_wait(&full[s], round & 1, abort_word, la.wait_cycles) ||
                         (PAIR && !wait_x(&pfull[s], round & 1, abort_word))) {
                         raise_abort();
+                        stop = true;
                         break;
                     }
                     tc::fence_after_sync();
@@ -459,14 +531,21 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
             }
         } else if (lane == 0 && PAIR) {
             // ---------------- relay (odd CTA of a pair) ----------------
-            uint32_t g = 0;
-            for (int u = unit0; u < la.nunits && !*abort_word; u += ustride) {
+            uint32_t g = 0, slot = 0;
+            bool stop = false;
+            while (!stop) {
+                const int u = take_unit(slot);
+                if (u < 0) {
+                    if (u == -2) raise_abort();
+                    break;
+                }
                 const int ktiles = unit_ktiles(la.tasks[la.units[u].task]);
                 for (int i = 0; i < ktiles; ++i, ++g) {
                     const int s = g % C::STAGES;
                     const uint32_t round = g / C::STAGES;
                     if (!tc::mbar_wait(&full[s], round & 1, abort_word, la.wait_cycles)) {
                         raise_abort();
+                        stop = true;
                         break;
                     }
                     tc::mbar_arrive_remote(tc::peer_smem(&pfull[s], 0));
@@ -478,8 +557,15 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
         const int quarter = warp & 3, half = warp >> 2;
         const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
         const uint32_t acce0 = PAIR ? tc::peer_smem(&acce[0], 0) : tc::smem_u32(&acce[0]);
-        uint32_t g = 0;
-        for (int u = unit0; u < la.nunits; u += ustride) {
+        uint32_t g = 0, slot = 0;
+        for (;;) {
+            int u = 0;
+            if (lane == 0) u = take_unit(slot);
+            u = __shfl_sync(0xffffffffu, u, 0);
+            if (u < 0) {
+                if (u == -2 && lane == 0) raise_abort();
+                break;
+            }
             const TcUnit un = la.units[u];
             const TcTask t = la.tasks[un.task];
             const int fills = (unit_ktiles(t) + la.kchain - 1) / la.kchain;
@@ -576,7 +662,7 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                 const bool k_ok = k0 < KTv * 64;
                 const int kt = k0 >> 6;
                 const uint32_t kin = (uint32_t)(k0 & 63);
-                uint8_t *tbuf = pa->buf[la.t_buf];
+                uint8_t *tbuf = pa->buf[t.t_buf];
                 const int NT = pa->NT;
 #pragma unroll
                 for (int g8 = 0; g8 < C::COLS / 8; ++g8) {
@@ -709,16 +795,19 @@ int tile_width(int code) { return code & (MXB_TILE_PAIR - 1); }
 bool tile_pair(int code) { return (code & MXB_TILE_PAIR) != 0; }
 
 // Position of an op in the evaluation sequence; ops of different plans with the same key run
-// in one launch.  W split, up-sweep by height, then for every depth far followed by down,
-// then near, then leaf down.
-enum OpPhase { PH_SPLITW = 0, PH_UP = 1, PH_FAR = 2, PH_DOWN = 3, PH_NEAR = 4, PH_LEAFDOWN = 5 };
+// in one launch.  W split, up-sweep by height, then the far couplings of every depth (they read
+// only the finished up-sweep) together with the near field when both use the same product
+// count, the downward transfers by depth, the near field otherwise, then leaf down.  Phase
+// values are the MXB_PHASE_* codes of the profiling API.
+enum OpPhase { PH_SPLITW = 0, PH_UP = 1, PH_FAR = 2, PH_DOWN = 3, PH_NEAR = 4, PH_LEAFDOWN = 5, PH_FARNEAR = 8 };
 int64_t op_key(int phase, int level)
 {
     switch (phase) {
     case PH_SPLITW: return 0;
     case PH_UP: return 1 + level;
-    case PH_FAR: return 100000 + 2 * (int64_t)level;
-    case PH_DOWN: return 100000 + 2 * (int64_t)level + 1;
+    case PH_FAR:
+    case PH_FARNEAR: return 100000;
+    case PH_DOWN: return 100000 + 1 + (int64_t)level;
     case PH_NEAR: return 10000000;
     default: return 10000001;
     }
@@ -727,7 +816,6 @@ int64_t op_key(int phase, int level)
 struct Op {             // one op of one plan
     int64_t key;
     int phase, level, P;
-    int a_pool, b_buf, t_buf;
     int first, count;   // range in the plan's tasks (TC) or jobs (W split)
 };
 
@@ -763,7 +851,7 @@ struct Batch : public mxb_batch {
     std::vector<Plan *> plans;
     struct MOp {
         int64_t key;
-        int phase, level, P, a_pool, b_buf, t_buf;
+        int phase, level, P;
         int first, count;  // range in the merged tasks or jobs
         int max_kt;
         int max_m;         // tallest output block (pairs only pay off above 128 rows)
@@ -775,6 +863,7 @@ struct Batch : public mxb_batch {
     TcTask *dTasks = nullptr;
     TcItem *dItems = nullptr;
     SplitJob *dJobs = nullptr;
+    int *dNext = nullptr;  // work-unit counter per op
     std::vector<void *> allocations;
     struct Entry {                     // one captured evaluation
         std::vector<const double *> W;
@@ -848,9 +937,6 @@ int Batch::build(const std::vector<Plan *> &ps)
         m.phase = o0->phase;
         m.level = o0->level;
         m.P = o0->P;
-        m.a_pool = o0->a_pool;
-        m.b_buf = o0->b_buf;
-        m.t_buf = o0->t_buf;
         m.max_kt = 1;
         m.max_m = 0;
         if (m.phase == PH_SPLITW) {
@@ -881,7 +967,7 @@ int Batch::build(const std::vector<Plan *> &ps)
                 }
             }
             m.count = (int)tasks.size() - m.first;
-            // longest tasks first: balances the persistent kernel's static round-robin
+            // longest tasks first: the kernel's CTAs claim units in this order (list scheduling)
             auto cost = [&](const TcTask &t) {
                 int k = 0;
                 for (int q = 0; q < t.nitem; ++q) k += items[t.item0 + q].KT;
@@ -903,6 +989,11 @@ int Batch::build(const std::vector<Plan *> &ps)
     int rc = up((void **)&dTasks, tasks.data(), tasks.size() * sizeof(TcTask));
     if (!rc) rc = up((void **)&dItems, items.data(), items.size() * sizeof(TcItem));
     if (!rc) rc = up((void **)&dJobs, jobs.data(), jobs.size() * sizeof(SplitJob));
+    if (!rc) {
+        cudaError_t e = cudaMalloc(&dNext, std::max<size_t>(ops.size(), 1) * sizeof(int));
+        if (e != cudaSuccess) return batch_fail(std::string("batch allocation: ") + cudaGetErrorString(e), MXB_ERR_NOMEM);
+        allocations.push_back(dNext);
+    }
     return rc;
 }
 
@@ -943,6 +1034,10 @@ int Batch::enqueue(Entry &e, cudaStream_t stream, int debug_flags, long long wai
     bool first_tc = true;
     int maxnt = 0;
     for (Plan *p : plans) maxnt = std::max(maxnt, p->bf16->nt_cap);
+    // work-unit counters of the tensor-core launches start at zero
+    cudaError_t zerr = only_op < 0 ? cudaMemsetAsync(dNext, 0, ops.size() * sizeof(int), stream)
+                                   : cudaMemsetAsync(dNext + only_op, 0, sizeof(int), stream);
+    if (zerr != cudaSuccess) return batch_fail(std::string("work-unit counters: ") + cudaGetErrorString(zerr), MXB_ERR_CUDA);
     for (size_t k = 0; k < ops.size(); ++k) {
         const MOp &m = ops[k];
         const bool run = only_op < 0 || (int)k == only_op;
@@ -960,9 +1055,7 @@ int Batch::enqueue(Entry &e, cudaStream_t stream, int debug_flags, long long wai
                 a.items = dItems;
                 a.units = e.dUnits + e.unit_first[k];
                 a.nunits = e.unit_count[k];
-                a.a_pool = m.a_pool;
-                a.b_buf = m.b_buf;
-                a.t_buf = m.t_buf < 0 ? 0 : m.t_buf;
+                a.next_unit = dNext + k;
                 a.err = plans[0]->bf16->dErr;
                 a.wait_cycles = wait_cycles > 0 ? wait_cycles : tc::WAIT_CYCLES;
                 a.stall_test = (debug_flags & MXB_DEBUG_STALL_ONE_WAIT) && first_tc;
@@ -1419,15 +1512,12 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
         maxh = std::max(maxh, height[v]);
         maxd = std::max(maxd, depth[v]);
     }
-    auto begin_op = [&](int phase, int level, int P, int a_pool, int b_buf, int t_buf) {
+    auto begin_op = [&](int phase, int level, int P) {
         Op o{};
         o.key = op_key(phase, level);
         o.phase = phase;
         o.level = level;
         o.P = P;
-        o.a_pool = a_pool;
-        o.b_buf = b_buf;
-        o.t_buf = t_buf;
         o.first = phase == PH_SPLITW ? (int)S->jobs.size() : (int)S->tasks.size();
         S->ops.push_back(o);
     };
@@ -1437,7 +1527,7 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
         if (o.count == 0) S->ops.pop_back();
     };
     auto add_tasks = [&](int16_t out_kind, int64_t c_row, int64_t out_kt, int ldc, int M, int item0,
-                         int16_t beta) {
+                         int16_t beta, int t_buf) {
         for (int m0 = 0; m0 < M; m0 += 128) {
             TcTask t{};
             t.c_row = c_row;
@@ -1450,12 +1540,15 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
             t.plan = 0;
             t.out_kind = out_kind;
             t.beta = beta;
+            t.t_buf = t_buf;
             S->tasks.push_back(t);
         }
     };
-    auto item = [&](uint64_t a_off, int64_t b_base, int K) {
+    auto item = [&](int a_pool, uint64_t a_off, int b_buf, int64_t b_base, int K) {
         TcItem it{};
+        it.a_pool = (int16_t)a_pool;
         it.a_off = a_off;
+        it.b_buf = (int16_t)b_buf;
         it.b_base = b_base;
         it.KT = KT(K);
         it.K = K;
@@ -1463,7 +1556,7 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
     };
 
     // W -> tiles
-    begin_op(PH_SPLITW, 0, 0, -1, BUF_W, -1);
+    begin_op(PH_SPLITW, 0, 0);
     for (int i = 0; i < nleaf; ++i) {
         SplitJob j{};
         j.src_row = i;
@@ -1477,63 +1570,72 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
     end_op();
     // up-sweep by height: the epilogue writes wskel directly as operand tiles
     for (int h = 0; h <= maxh; ++h) {
-        begin_op(PH_UP, h, 3, POOL_VU3, h == 0 ? BUF_W : BUF_WSKEL, BUF_WSKEL);
+        begin_op(PH_UP, h, 3);
         for (int v : bfs) {
             if (height[v] != h || !projects(v)) continue;
             const int item0 = (int)S->items.size();
             if (lch[v] == -1) {
-                item(up_a[v], S->leaf_kt[lm[v]], Ddim[lm[v]]);
+                item(POOL_VU3, up_a[v], BUF_W, S->leaf_kt[lm[v]], Ddim[lm[v]]);
             } else {
-                if (slen[lch[v]] > 0) item(up_a[v], S->node_kt[lch[v]], slen[lch[v]]);
-                if (slen[rch[v]] > 0) item(up_b[v], S->node_kt[rch[v]], slen[rch[v]]);
+                if (slen[lch[v]] > 0) item(POOL_VU3, up_a[v], BUF_WSKEL, S->node_kt[lch[v]], slen[lch[v]]);
+                if (slen[rch[v]] > 0) item(POOL_VU3, up_b[v], BUF_WSKEL, S->node_kt[rch[v]], slen[rch[v]]);
             }
-            add_tasks(OUT_TILES, skel_row[v], S->node_kt[v], slen[v], slen[v], item0, 0);
+            add_tasks(OUT_TILES, skel_row[v], S->node_kt[v], slen[v], slen[v], item0, 0, BUF_WSKEL);
         }
         end_op();
     }
-    // far + down by depth: a node whose parent projects keeps its far result in FP32 for the
-    // down launch, which adds its own product and writes uskel tiles; other nodes' far
-    // results become tiles directly
+    // far couplings of every depth in one launch (they read only wskel): a node whose parent
+    // projects keeps its far result in FP32 for its down launch, which adds its own product and
+    // writes uskel tiles; other nodes' far results become tiles directly.  The near field
+    // (Y (+)= D W, reads only W) joins that launch when it uses the same product count.
     auto has_down = [&](int c) { return parent[c] >= 0 && projects(parent[c]); };
     std::vector<std::vector<int>> far_out(numnodes);
     for (size_t k = 0; k < far_x.size(); ++k) far_out[far_x[k]].push_back((int)k);
-    for (int dd = 1; dd <= maxd; ++dd) {
-        begin_op(PH_FAR, dd, far_parts, POOL_FAR, BUF_WSKEL, BUF_USKEL);
-        for (int c : bfs) {
-            if (depth[c] != dd || !projects(c)) continue;
+    std::vector<std::vector<int>> near_out(nleaf);
+    for (size_t k = 0; k < near_x.size(); ++k) near_out[near_x[k]].push_back((int)k);
+    auto near_tasks = [&]() {
+        for (int v : bfs) {
+            if (lch[v] != -1) continue;
+            const int x = lm[v];
             const int item0 = (int)S->items.size();
-            for (int k : far_out[c])
-                if (slen[far_y[k]] > 0) item(far_a[k], S->node_kt[far_y[k]], slen[far_y[k]]);
-            add_tasks(has_down(c) ? OUT_F32 : OUT_TILES, skel_row[c], S->node_kt[c], slen[c], slen[c], item0, 0);
+            for (int k : near_out[x]) item(POOL_NEAR, near_a[k], BUF_W, S->leaf_kt[near_y[k]], Ddim[near_y[k]]);
+            add_tasks(OUT_Y, x, 0, Ddim[x], Ddim[x], item0, 2, BUF_W);
         }
-        end_op();
-        begin_op(PH_DOWN, dd, 3, POOL_VD3, BUF_USKEL, BUF_USKEL);
+    };
+    const bool near_with_far = near_parts == far_parts;
+    begin_op(near_with_far ? PH_FARNEAR : PH_FAR, 0, far_parts);
+    for (int c : bfs) {
+        if (!projects(c)) continue;
+        const int item0 = (int)S->items.size();
+        for (int k : far_out[c])
+            if (slen[far_y[k]] > 0) item(POOL_FAR, far_a[k], BUF_WSKEL, S->node_kt[far_y[k]], slen[far_y[k]]);
+        add_tasks(has_down(c) ? OUT_F32 : OUT_TILES, skel_row[c], S->node_kt[c], slen[c], slen[c], item0, 0,
+                  BUF_USKEL);
+    }
+    if (near_with_far) near_tasks();
+    end_op();
+    for (int dd = 1; dd <= maxd; ++dd) {
+        begin_op(PH_DOWN, dd, 3);
         for (int c : bfs) {
             if (depth[c] != dd || !projects(c) || !has_down(c)) continue;
             const int item0 = (int)S->items.size();
-            item(down_child[c], S->node_kt[parent[c]], slen[parent[c]]);
-            add_tasks(OUT_TILES, skel_row[c], S->node_kt[c], slen[c], slen[c], item0, 1);
+            item(POOL_VD3, down_child[c], BUF_USKEL, S->node_kt[parent[c]], slen[parent[c]]);
+            add_tasks(OUT_TILES, skel_row[c], S->node_kt[c], slen[c], slen[c], item0, 1, BUF_USKEL);
         }
         end_op();
     }
-    // near (Y (+)= D W) then leaf down (Y += P^T uskel)
-    std::vector<std::vector<int>> near_out(nleaf);
-    for (size_t k = 0; k < near_x.size(); ++k) near_out[near_x[k]].push_back((int)k);
-    begin_op(PH_NEAR, 0, near_parts, POOL_NEAR, BUF_W, -1);
-    for (int v : bfs) {
-        if (lch[v] != -1) continue;
-        const int x = lm[v];
-        const int item0 = (int)S->items.size();
-        for (int k : near_out[x]) item(near_a[k], S->leaf_kt[near_y[k]], Ddim[near_y[k]]);
-        add_tasks(OUT_Y, x, 0, Ddim[x], Ddim[x], item0, 2);
+    // near (if not with the far couplings), then leaf down (Y += P^T uskel)
+    if (!near_with_far) {
+        begin_op(PH_NEAR, 0, near_parts);
+        near_tasks();
+        end_op();
     }
-    end_op();
-    begin_op(PH_LEAFDOWN, 0, 3, POOL_VD3, BUF_USKEL, -1);
+    begin_op(PH_LEAFDOWN, 0, 3);
     for (int v : bfs) {
         if (lch[v] != -1 || !projects(v)) continue;
         const int item0 = (int)S->items.size();
-        item(down_a[v], S->node_kt[v], slen[v]);
-        add_tasks(OUT_Y, lm[v], 0, Ddim[lm[v]], Ddim[lm[v]], item0, 1);
+        item(POOL_VD3, down_a[v], BUF_USKEL, S->node_kt[v], slen[v]);
+        add_tasks(OUT_Y, lm[v], 0, Ddim[lm[v]], Ddim[lm[v]], item0, 1, BUF_W);
     }
     end_op();
 

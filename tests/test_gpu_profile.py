@@ -19,7 +19,7 @@ def torch():
     return t
 
 
-@pytest.mark.parametrize("precision", ["fp64", "split_bf16", "split_bf16_x6"])
+@pytest.mark.parametrize("precision", ["fp64", "split_bf16", "split_bf16_far6", "split_bf16_x6"])
 @pytest.mark.parametrize("name", ["hss", "h2b", "ragged"])
 def test_profile_flops_and_result(torch, small_cases, name, precision):
     cds = small_cases[name]
@@ -43,7 +43,11 @@ def test_profile_flops_and_result(torch, small_cases, name, precision):
     if precision == "fp64":
         assert phases <= {"up", "far_down", "near_leaf_down"}
     else:
-        assert phases <= {"split_w", "up", "far", "down", "near", "leaf_down"}
+        assert phases <= {"split_w", "up", "far", "far_near", "down", "near", "leaf_down"}
+        # the far couplings of all depths run as one launch, joined by the near field when
+        # both use the same number of products
+        assert sum(x["phase"] in ("far", "far_near") for x in recs) == 1
+        assert ("near" in phases) == (precision == "split_bf16_far6")
         k = 6.0 if precision == "split_bf16_x6" else None
         if k:
             for x in recs:
