@@ -43,7 +43,59 @@ def parse():
     ap.add_argument("--nrhs", type=int, default=None)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--tolerance-sweep", action="store_true",
+                    help="accuracy report instead of the benchmark: the same points and kernel compressed "
+                         "at ID tolerances 1e-3, 1e-5 and 1e-7, FP64 and split-BF16 (one JSON line each)")
     return ap.parse_args()
+
+
+def tolerance_sweep(args, cfg):
+    """Relative error of the FP64 and split-BF16 evaluators against the dense FP64 K W (64
+    sampled rows) and of split-BF16 against FP64 on the same CDS, at three ID tolerances."""
+    import torch
+    from matrox_ru_b200 import build as mbuild, hgemm as H, structure as S
+    mbuild.build()
+    dev = torch.device("cuda", 0)
+    X = S.gaussian_mixture(cfg["n"], cfg["d"], cfg["components"], *cfg["mean_range"], *cfg["sigma_range"],
+                           seed=cfg["seed"])
+    spec = S.KernelSpec(cfg["kernel"], cfg["h"])
+    r = cfg["nrhs"]
+    for tol in (1e-3, 1e-5, 1e-7):
+        cds = S.build_cds(X, spec, leaf_size=cfg["leaf"], budget=cfg["budget"], tol=tol, max_rank=cfg["max_rank"],
+                          seed=cfg["seed"])
+        g = torch.Generator(device=dev).manual_seed(cfg["seed"] + 1)
+        TW = torch.randn(cds.n * r, dtype=torch.float64, device=dev, generator=g)
+        rows = np.random.default_rng(0).choice(cds.n, 64, replace=False)
+        dense = S.dense_kernel_times(X, cds.from_tree_order(TW.cpu().numpy(), r), spec, rows=rows)
+        line = {"report": "accuracy across compression tolerances", "tol": tol, "nrhs": r,
+                "workload": cfg["workload"].replace("tol 1e-5", f"tol {tol:g}"),
+                "ranks": {"min": int(cds.slen[cds.slen > 0].min()), "median": float(np.median(cds.slen[cds.slen > 0])),
+                          "max": int(cds.slen.max())},
+                "flops_per_eval": cds.flops(r)}
+        outs = {}
+        for mode in ("fp64", "split_bf16"):
+            plan = H.Plan(cds, mode)
+            out = torch.zeros_like(TW)
+            for _ in range(3):
+                plan.evaluate(TW, r, out=out)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(args.steps):
+                plan.evaluate(TW, r, out=out)
+            e1.record()
+            e1.synchronize()
+            plan.status()
+            Y = out.cpu().numpy()
+            outs[mode] = Y
+            line[mode] = {"ms": round(e0.elapsed_time(e1) / args.steps, 4),
+                          "rel_err_vs_dense_64rows": float(np.linalg.norm(cds.from_tree_order(Y, r)[rows] - dense)
+                                                           / np.linalg.norm(dense))}
+            del plan, out
+            torch.cuda.empty_cache()
+        line["split_bf16"]["rel_err_vs_fp64_same_cds"] = float(np.linalg.norm(outs["split_bf16"] - outs["fp64"])
+                                                               / np.linalg.norm(outs["fp64"]))
+        print(json.dumps(line), flush=True)
 
 
 def build_cds(cfg):
@@ -204,6 +256,9 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.tolerance_sweep:
+        tolerance_sweep(args, cfg)
+        return
     if args.impl == "reference":
         if world > 1:
             import torch.distributed as dist
