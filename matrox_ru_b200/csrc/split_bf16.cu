@@ -569,6 +569,33 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
             const TcUnit un = la.units[u];
             const TcTask t = la.tasks[un.task];
             const int fills = (unit_ktiles(t) + la.kchain - 1) / la.kchain;
+            {
+                // The output phase reads old values (Y, the far result) with a few loads in
+                // flight per thread: ask L2 for them now, so the unit's MMAs cover the DRAM
+                // latency.  Lane j takes columns j, j + 32, ... of its warp's 32-row segment
+                // (128 bytes of FP32, 256 of FP64 per column).
+                const PlanArgs *pa = la.plans + t.plan;
+                const int r0 = t.m0 + (int)rank * 128 + quarter * 32;
+                const int c0 = un.col * BN + half * C::COLS;
+                const int beta = t.beta == 2 ? pa->beta_arg : t.beta;
+                const int nrhs = pa->nrhs;
+                const char *f32 = nullptr, *f64 = nullptr;
+                if (t.out_kind == OUT_Y && beta) f64 = reinterpret_cast<const char *>(pa->Y + pa->yofs[t.c_row] + r0);
+                else if (t.out_kind == OUT_TILES && beta)
+                    f32 = reinterpret_cast<const char *>(pa->skel + t.c_row * (int64_t)nrhs + r0);
+                if (r0 < t.M && (f32 || f64)) {
+                    for (int j = lane; j < C::COLS; j += 32) {
+                        const int cc = c0 + j;
+                        if (cc >= nrhs) break;
+                        if (f32) asm volatile("prefetch.global.L2 [%0];\n" ::"l"(f32 + (size_t)cc * t.ldc * 4));
+                        if (f64) {  // rows r0 and r0 + 16 (only where they exist)
+                            const char *q = f64 + (size_t)cc * t.ldc * 8;
+                            asm volatile("prefetch.global.L2 [%0];\n" ::"l"(q));
+                            if (r0 + 16 < t.M) asm volatile("prefetch.global.L2 [%0];\n" ::"l"(q + 128));
+                        }
+                    }
+                }
+            }
             float acc[C::COLS];
 #pragma unroll
             for (int e = 0; e < C::COLS; ++e) acc[e] = 0.f;
