@@ -252,6 +252,9 @@ struct TcCfg {
     static constexpr int RING_READERS = PAIR ? 2 * (1 + EPI_WARPS) + 1 : 1 + EPI_WARPS;
     static constexpr int THREADS = (EPI_WARPS + 2) * 32;
     static constexpr int COLS = BN / 2;          // accumulator columns per epilogue thread
+    // old values loaded ahead of the stores in the epilogue's read-modify-writes (fewer where
+    // 128 accumulators already fill the registers)
+    static constexpr int RMW = COLS >= 128 ? 8 : 16;
     static constexpr int NACC = BN >= 256 ? 2 : 4;  // TMEM accumulator buffers (512 columns at most)
     static constexpr int TMEM_COLS = NACC * BN;
     static constexpr int M_MMA = PAIR ? 256 : 128;
@@ -610,14 +613,15 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                 }
                 tc::fence_after_sync();
                 // 64 columns per load where the registers allow (one wait per 64 columns keeps
-                // the drain short); 128-column halves keep 32 to stay clear of spills
-                constexpr int LB = C::COLS == 64 ? 64 : 32;
+                // the drain short); 128-column halves load 16 at a time to stay clear of spills
+                constexpr int LB = C::COLS == 64 ? 64 : (C::COLS >= 128 ? 16 : 32);
 #pragma unroll
                 for (int c0 = 0; c0 < C::COLS; c0 += LB) {
                     float v[LB];
                     const uint32_t ta = tmem + lane_base + (uint32_t)(b * BN + half * C::COLS + c0);
                     if constexpr (LB == 64) tc::tmem_ld64(ta, v);
-                    else tc::tmem_ld32(ta, v);
+                    else if constexpr (LB == 32) tc::tmem_ld32(ta, v);
+                    else tc::tmem_ld16(ta, v);
 #pragma unroll
                     for (int e = 0; e < LB; ++e) acc[c0 + e] += v[e];
                 }
@@ -641,15 +645,15 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                 if (r < t.M) {
                     double *Yb = pa->Y + pa->yofs[t.c_row] + r;
 #pragma unroll
-                    for (int c0 = 0; c0 < C::COLS; c0 += 16) {
-                        double old[16];
+                    for (int c0 = 0; c0 < C::COLS; c0 += C::RMW) {
+                        double old[C::RMW];
 #pragma unroll
-                        for (int e = 0; e < 16; ++e) {
+                        for (int e = 0; e < C::RMW; ++e) {
                             const int cc = col0 + c0 + e;
                             old[e] = (beta && cc < nrhs) ? Yb[(size_t)cc * t.ldc] : 0.0;
                         }
 #pragma unroll
-                        for (int e = 0; e < 16; ++e) {
+                        for (int e = 0; e < C::RMW; ++e) {
                             const int cc = col0 + c0 + e;
                             if (cc < nrhs) Yb[(size_t)cc * t.ldc] = old[e] + (double)acc[c0 + e];
                         }
@@ -673,15 +677,15 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                 if (beta && r < t.M) {
                     const float *Sb = pa->skel + t.c_row * (int64_t)nrhs + r;
 #pragma unroll
-                    for (int c0 = 0; c0 < C::COLS; c0 += 16) {
-                        float old[16];
+                    for (int c0 = 0; c0 < C::COLS; c0 += C::RMW) {
+                        float old[C::RMW];
 #pragma unroll
-                        for (int e = 0; e < 16; ++e) {
+                        for (int e = 0; e < C::RMW; ++e) {
                             const int cc = col0 + c0 + e;
                             old[e] = cc < nrhs ? Sb[(size_t)cc * t.ldc] : 0.f;
                         }
 #pragma unroll
-                        for (int e = 0; e < 16; ++e) acc[c0 + e] += old[e];
+                        for (int e = 0; e < C::RMW; ++e) acc[c0 + e] += old[e];
                     }
                 }
                 const int KTv = (t.M + 63) / 64;
