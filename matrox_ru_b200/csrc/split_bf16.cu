@@ -95,6 +95,8 @@ struct TcTask {
 struct TcUnit {
     int32_t task;
     int32_t col;     // column tile: right-hand sides [col * BN, col * BN + BN)
+    int32_t ktiles;  // K tiles of the task (sum over its items)
+    int32_t pad;
 };
 
 struct SplitJob {     // one leaf block of W -> B-operand tiles
@@ -296,7 +298,8 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
     uint64_t *ufull = doneb + 1;          // ring slot i holds a unit
     uint64_t *uempty = ufull + RING;      // every reader of ring slot i has taken its unit
     volatile int *ring = reinterpret_cast<volatile int *>(uempty + RING);
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(const_cast<int *>(ring) + RING);
+    volatile int *ring_kt = ring + RING;  // K tiles of the unit in ring slot i
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(const_cast<int *>(ring_kt) + RING);
     volatile int *abort_word = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -314,14 +317,18 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
     auto arrive_local = [&](uint64_t *bar) {
         asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(tc::smem_u32(bar)) : "memory");
     };
-    // Next unit of the ring for a reader (one thread): waits for slot `slot`, takes the unit
-    // and releases the slot to the producer (in the even CTA of a pair).  -2: a wait gave up.
-    auto take_unit = [&](uint32_t &slot) -> int {
+    // Next unit of the ring for a reader (one thread): waits for slot `slot`, takes the unit and
+    // its K-tile count and releases the slot to the producer (in the even CTA of a pair).
+    // -2: a wait gave up.
+    auto take_unit = [&](uint32_t &slot, int &ktiles) -> int {
         const int i = (int)(slot % RING);
         const uint32_t parity = (slot / RING) & 1u;
         ++slot;
         int u = -2;
-        if (wait_x(&ufull[i], parity, abort_word)) u = ring[i];
+        if (wait_x(&ufull[i], parity, abort_word)) {
+            u = ring[i];
+            ktiles = ring_kt[i];
+        }
         if constexpr (PAIR) {
             if (rank == 1) tc::mbar_arrive_remote(tc::peer_smem(&uempty[i], 0));
             else arrive_local(&uempty[i]);
@@ -359,12 +366,6 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
     tc::fence_after_sync();
     const uint32_t tmem = *tmem_slot;
 
-    auto unit_ktiles = [&](const TcTask &t) {
-        int k = 0;
-        for (int q = 0; q < t.nitem; ++q) k += la.items[t.item0 + q].KT;
-        return k;
-    };
-
     if (warp == C::EPI_WARPS) {
         if (lane == 0) {
             // ---------------- producer ----------------
@@ -375,11 +376,12 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
             for (int s = 0; s < C::STAGES; ++s) filled[s] = 0;
             bool stop = false;
             while (!stop && !*abort_word) {
-                int u;
+                int u, kt_unit = 0;
                 if (!PAIR || issuer) {
                     // claim the next unit and publish it to every reader
                     u = atomicAdd(la.next_unit, 1);
                     if (u >= la.nunits) u = -1;
+                    if (u >= 0) kt_unit = la.units[u].ktiles;
                     const int i = (int)(slot % RING);
                     const uint32_t round = slot / RING;
                     ++slot;
@@ -388,13 +390,15 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                         break;
                     }
                     ring[i] = u;
+                    ring_kt[i] = kt_unit;
                     if constexpr (PAIR) {
                         tc::st_remote_u32(tc::peer_smem((const void *)&ring[i], 1), (uint32_t)u);
+                        tc::st_remote_u32(tc::peer_smem((const void *)&ring_kt[i], 1), (uint32_t)kt_unit);
                         tc::mbar_arrive_remote(tc::peer_smem(&ufull[i], 1));
                     }
                     arrive_local(&ufull[i]);
                 } else {
-                    u = take_unit(slot);
+                    u = take_unit(slot, kt_unit);
                     if (u == -2) {
                         raise_abort();
                         break;
@@ -478,12 +482,12 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
             uint32_t slot = 0;  // ring counter
             bool any = false, stop = false;
             while (!stop) {
-                const int u = take_unit(slot);
+                int ktiles = 0;
+                const int u = take_unit(slot, ktiles);
                 if (u < 0) {
                     if (u == -2) raise_abort();
                     break;
                 }
-                const int ktiles = unit_ktiles(la.tasks[la.units[u].task]);
                 for (int i = 0; i < ktiles; ++i, ++g) {
                     const int s = g % C::STAGES;
                     const uint32_t round = g / C::STAGES;
@@ -499,16 +503,18 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                         break;
                     }
                     tc::fence_after_sync();
+                    // descriptors of the stage's part tiles; a byte offset o within the stage adds
+                    // o >> 4 to the start-address field (shared addresses stay below 2^18)
                     const uint32_t sa = tc::smem_u32(smem + s * C::STAGE);
-                    const uint32_t sb = sa + C::A_BYTES;
+                    const uint64_t da = tc::smem_desc_sw128(sa), db = tc::smem_desc_sw128(sa + C::A_BYTES);
                     const uint32_t dst = tmem + (uint32_t)(b * BN);
                     uint32_t accum = first ? 0u : 1u;
 #pragma unroll
                     for (int ks = 0; ks < 4; ++ks) {
 #pragma unroll
                         for (int j = 0; j < C::NPROD; ++j) {
-                            const uint64_t ad = tc::smem_desc_sw128(sa + PA[j] * TILE_BYTES + ks * 32);
-                            const uint64_t bd = tc::smem_desc_sw128(sb + PB[j] * C::B_ROWS_BYTES + ks * 32);
+                            const uint64_t ad = da + (uint64_t)((PA[j] * TILE_BYTES + ks * 32) >> 4);
+                            const uint64_t bd = db + (uint64_t)((PB[j] * C::B_ROWS_BYTES + ks * 32) >> 4);
                             if constexpr (PAIR) tc::mma_bf16_pair(dst, ad, bd, IDESC, accum);
                             else tc::mma_bf16(dst, ad, bd, IDESC, accum);
                             accum = 1;
@@ -537,12 +543,12 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
             uint32_t g = 0, slot = 0;
             bool stop = false;
             while (!stop) {
-                const int u = take_unit(slot);
+                int ktiles = 0;
+                const int u = take_unit(slot, ktiles);
                 if (u < 0) {
                     if (u == -2) raise_abort();
                     break;
                 }
-                const int ktiles = unit_ktiles(la.tasks[la.units[u].task]);
                 for (int i = 0; i < ktiles; ++i, ++g) {
                     const int s = g % C::STAGES;
                     const uint32_t round = g / C::STAGES;
@@ -562,16 +568,17 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
         const uint32_t acce0 = PAIR ? tc::peer_smem(&acce[0], 0) : tc::smem_u32(&acce[0]);
         uint32_t g = 0, slot = 0;
         for (;;) {
-            int u = 0;
-            if (lane == 0) u = take_unit(slot);
+            int u = 0, ktiles = 0;
+            if (lane == 0) u = take_unit(slot, ktiles);
             u = __shfl_sync(0xffffffffu, u, 0);
+            ktiles = __shfl_sync(0xffffffffu, ktiles, 0);
             if (u < 0) {
                 if (u == -2 && lane == 0) raise_abort();
                 break;
             }
             const TcUnit un = la.units[u];
             const TcTask t = la.tasks[un.task];
-            const int fills = (unit_ktiles(t) + la.kchain - 1) / la.kchain;
+            const int fills = (ktiles + la.kchain - 1) / la.kchain;
             {
                 // The output phase reads old values (Y, the far result) with a few loads in
                 // flight per thread: ask L2 for them now, so the unit's MMAs cover the DRAM
@@ -1042,7 +1049,9 @@ int Batch::units_for(Entry &e, const std::vector<int> &bn)
         for (int t = m.first; t < m.first + m.count; ++t) {
             if (pair && tasks[t].m0 % 256) continue;  // the pair's odd CTA takes rows m0 + 128
             const int ncol = (int)ceil_div(e.nrhs[tasks[t].plan], tile_width(bn[k]));
-            for (int c = 0; c < ncol; ++c) units.push_back(TcUnit{t, c});
+            int kt = 0;
+            for (int q = tasks[t].item0; q < tasks[t].item0 + tasks[t].nitem; ++q) kt += items[q].KT;
+            for (int c = 0; c < ncol; ++c) units.push_back(TcUnit{t, c, kt, 0});
         }
         e.unit_count[k] = (int)units.size() - e.unit_first[k];
     }
