@@ -407,6 +407,10 @@ int Plan::create(const mxb_cds_desc &d, int prec, Plan **out)
         rc = p->setup_split_bf16(d);
         if (rc) return rc;
     }
+    // The uploads above are synchronous copies from pageable memory, which may return before
+    // their DMA has landed; the evaluations that follow run on the caller's streams, which do
+    // not wait for the legacy stream.  Wait for every copy here.
+    MXB_CUDA(cudaDeviceSynchronize());
     *out = p.release();
     return MXB_OK;
 }

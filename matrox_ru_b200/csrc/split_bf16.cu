@@ -945,7 +945,7 @@ struct Batch : public mxb_batch {
                  int debug_flags, long long wait_cycles);
     int enqueue(Entry &e, cudaStream_t stream, int debug_flags, long long wait_cycles, const std::vector<int> &bn,
                 int only_op = -1);
-    int units_for(Entry &e, const std::vector<int> &bn);
+    int units_for(Entry &e, const std::vector<int> &bn, cudaStream_t stream);
     int tune(Entry &e, std::vector<PlanArgs> pa, std::vector<int> &bn, cudaStream_t stream, long long wait_cycles);
     Entry *find(const double *const *W, double *const *Y, const std::vector<int> &nr, int accumulate,
                 int debug_flags);
@@ -1032,11 +1032,15 @@ int Batch::build(const std::vector<Plan *> &ps)
         if (e != cudaSuccess) return batch_fail(std::string("batch allocation: ") + cudaGetErrorString(e), MXB_ERR_NOMEM);
         allocations.push_back(dNext);
     }
+    // synchronous copies from pageable memory may return before their DMA lands, and the
+    // evaluations run on streams that do not wait for the legacy stream
+    if (!rc && cudaDeviceSynchronize() != cudaSuccess) rc = batch_fail("batch upload: synchronisation failed", MXB_ERR_CUDA);
     return rc;
 }
 
 // Work units of every TC op for this entry's nrhs and column-tile choices.
-int Batch::units_for(Entry &e, const std::vector<int> &bn)
+// The list is uploaded on `stream`, ahead of the launches that read it.
+int Batch::units_for(Entry &e, const std::vector<int> &bn, cudaStream_t stream)
 {
     std::vector<TcUnit> units;
     e.unit_first.assign(ops.size(), 0);
@@ -1059,7 +1063,7 @@ int Batch::units_for(Entry &e, const std::vector<int> &bn)
     e.dUnits = nullptr;
     cudaError_t err = cudaMalloc(&e.dUnits, std::max<size_t>(units.size(), 1) * sizeof(TcUnit));
     if (err == cudaSuccess && !units.empty())
-        err = cudaMemcpy(e.dUnits, units.data(), units.size() * sizeof(TcUnit), cudaMemcpyHostToDevice);
+        err = cudaMemcpyAsync(e.dUnits, units.data(), units.size() * sizeof(TcUnit), cudaMemcpyHostToDevice, stream);
     if (err != cudaSuccess) return batch_fail(std::string("work units: ") + cudaGetErrorString(err), MXB_ERR_CUDA);
     return MXB_OK;
 }
@@ -1215,14 +1219,14 @@ int Batch::tune(Entry &e, std::vector<PlanArgs> pa, std::vector<int> &bn, cudaSt
     }
     if (!rc && cudaMalloc(&dTune, np * sizeof(PlanArgs)) != cudaSuccess)
         rc = batch_fail("autotune table allocation failed", MXB_ERR_NOMEM);
-    if (!rc && cudaMemcpy(dTune, pa.data(), np * sizeof(PlanArgs), cudaMemcpyHostToDevice) != cudaSuccess)
+    if (!rc && cudaMemcpyAsync(dTune, pa.data(), np * sizeof(PlanArgs), cudaMemcpyHostToDevice, stream) != cudaSuccess)
         rc = batch_fail("autotune table upload failed", MXB_ERR_CUDA);
     te.dPlans = dTune;
     if (!rc && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
         rc = batch_fail("autotune events", MXB_ERR_CUDA);
     for (size_t k = 0; k < ops.size() && !rc; ++k) {
         if (ops[k].phase == PH_SPLITW) {
-            rc = units_for(te, bn);
+            rc = units_for(te, bn, stream);
             if (!rc) rc = enqueue(te, stream, 0, wait_cycles, bn, (int)k);
             continue;
         }
@@ -1237,7 +1241,7 @@ int Batch::tune(Entry &e, std::vector<PlanArgs> pa, std::vector<int> &bn, cudaSt
             if (tile_width(c) > 2 * std::max(64, maxn)) continue;
             std::vector<int> trial = bn;
             trial[k] = c;
-            rc = units_for(te, trial);
+            rc = units_for(te, trial, stream);
             float ms = 0.f;
             bool refused = false;
             for (int rep = 0; rep < 2 && !rc && !refused; ++rep) {
@@ -1262,7 +1266,7 @@ int Batch::tune(Entry &e, std::vector<PlanArgs> pa, std::vector<int> &bn, cudaSt
             }
         }
         bn[k] = best_bn;
-        if (!rc) rc = units_for(te, bn);
+        if (!rc) rc = units_for(te, bn, stream);
         if (!rc) rc = enqueue(te, stream, 0, wait_cycles, bn, (int)k);
     }
     if (!rc && cudaStreamSynchronize(stream) != cudaSuccess) rc = batch_fail("autotune sync", MXB_ERR_CUDA);
@@ -1323,7 +1327,9 @@ int Batch::evaluate(const double *const *W, double *const *Y, const int *nrhs, i
             pa[i].beta_arg = accumulate ? 1 : 0;
         }
         cudaError_t err = cudaMalloc(&e.dPlans, np * sizeof(PlanArgs));
-        if (err == cudaSuccess) err = cudaMemcpy(e.dPlans, pa.data(), np * sizeof(PlanArgs), cudaMemcpyHostToDevice);
+        // on the evaluation stream, ahead of the graph launch that reads it
+        if (err == cudaSuccess)
+            err = cudaMemcpyAsync(e.dPlans, pa.data(), np * sizeof(PlanArgs), cudaMemcpyHostToDevice, stream);
         if (err != cudaSuccess) {
             release(e);
             return batch_fail(std::string("batch plan table: ") + cudaGetErrorString(err), MXB_ERR_CUDA);
@@ -1348,7 +1354,7 @@ int Batch::evaluate(const double *const *W, double *const *Y, const int *nrhs, i
             tuned[nr] = bn;
         }
         e.bn = bn;
-        int rc = units_for(e, bn);
+        int rc = units_for(e, bn, stream);
         if (rc) {
             release(e);
             return rc;

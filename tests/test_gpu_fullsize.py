@@ -4,7 +4,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from matrox_ru_b200 import hgemm as H, structure as S
+from matrox_ru_b200 import _lib, hgemm as H, structure as S
 
 pytestmark = pytest.mark.gpu
 SEED = 20261203
@@ -75,3 +75,29 @@ def test_c1_split_bf16_full_columns(torch, c1, mode, tol):
     plan.status()
     err = (torch.linalg.norm(got - want) / torch.linalg.norm(want)).item()
     assert 1e-12 < err <= tol, err
+
+
+def test_c1_split_dropin_first_call(torch, c1):
+    """The first drop-in call creates the evaluation graphs of its slab buffers while earlier
+    slabs are in flight and the PCIe bus is busy with slab copies: every slab of that call
+    must match the plan API on all 1024 columns (the graphs' tables are uploaded in stream
+    order, ahead of the launches that read them)."""
+    r = 1024
+    W = torch.as_tensor(np.random.default_rng(3).standard_normal(c1.n * r), device="cuda")
+    want = H.Plan(c1, "split_bf16").evaluate(W, r).cpu().numpy()
+    tw = torch.empty(c1.n * r, dtype=torch.float64, pin_memory=True)
+    tw.copy_(W.cpu())
+    y = torch.zeros(c1.n * r, dtype=torch.float64, pin_memory=True)
+    H.cache_invalidate()
+    H.set_precision("split_bf16")
+    try:
+        for flags in (_lib.FLAG_OUTPUT_IS_ZERO, 0):
+            H.set_flags(flags)
+            y.zero_()
+            H.evaluate_host(c1, tw.numpy(), r, apres=y.numpy())
+            got = y.numpy()
+            assert np.abs(got - want).max() <= 1e-6 * np.abs(want).max(), flags
+    finally:
+        H.set_flags(0)
+        H.set_precision("fp64")
+        H.cache_invalidate()
