@@ -101,3 +101,38 @@ def test_c1_split_dropin_first_call(torch, c1):
         H.set_flags(0)
         H.set_precision("fp64")
         H.cache_invalidate()
+
+
+@pytest.fixture(scope="module")
+def hss_c0():
+    """HSS (near-field budget 0): N = 16384 points in d = 8 from an 8-component isotropic
+    mixture (means uniform in [0, 4]^8, sigma 0.5), Gaussian h = 1, leaf 128, ID tolerance
+    1e-5, max rank 128."""
+    X = S.gaussian_mixture(16384, 8, 8, 0.0, 4.0, 0.5, None, seed=SEED)
+    spec = S.KernelSpec("gaussian", 1.0)
+    return X, spec, S.build_cds(X, spec, leaf_size=128, budget=0.0, tol=1e-5, max_rank=128, seed=SEED)
+
+
+def test_hss_full_size_vs_reference(torch, hss_c0):
+    """The HSS drop-in on all 256 columns against the reference's own parHSSGEMM (FP64,
+    <= 1e-12), the split-BF16 path against FP64 (<= 1e-5), and both against the dense K W
+    on sampled rows (the compression error, the same for both)."""
+    X, spec, cds = hss_c0
+    assert cds.is_hss and cds.nleaf == 128
+    r = 256
+    TW = np.random.default_rng(8).standard_normal(cds.n * r)
+    got = H.evaluate_host(cds, TW, r)  # FP64 drop-in (parHSSGEMM signature)
+    if O.ref_available():
+        want = O.eval_h2b(cds, TW, r, use_reference=True)
+        assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max()
+    plan = H.Plan(cds, "split_bf16")
+    split = plan.evaluate(torch.as_tensor(TW, device="cuda"), r).cpu().numpy()
+    plan.status()
+    assert 1e-12 < np.linalg.norm(split - got) / np.linalg.norm(got) <= 1e-5
+    rows = np.random.default_rng(0).choice(cds.n, 64, replace=False)
+    dense = S.dense_kernel_times(X, cds.from_tree_order(TW, r), spec, rows=rows)
+    e64 = np.linalg.norm(cds.from_tree_order(got, r)[rows] - dense) / np.linalg.norm(dense)
+    es = np.linalg.norm(cds.from_tree_order(split, r)[rows] - dense) / np.linalg.norm(dense)
+    # HSS compression at max rank 128 leaves ~0.13 here (the ranks saturate); the split path
+    # must not add to it beyond its own arithmetic error
+    assert e64 < 0.5 and abs(es - e64) <= 1e-5, (e64, es)
