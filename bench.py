@@ -43,10 +43,85 @@ def parse():
     ap.add_argument("--nrhs", type=int, default=None)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--batched", action="store_true",
+                    help="report instead of the benchmark: 64 uneven H2-b matrices in one merged, "
+                         "graph-captured launch sequence vs the same plans evaluated one by one")
     ap.add_argument("--tolerance-sweep", action="store_true",
                     help="accuracy report instead of the benchmark: the same points and kernel compressed "
                          "at ID tolerances 1e-3, 1e-5 and 1e-7, FP64 and split-BF16 (one JSON line each)")
     return ap.parse_args()
+
+
+def batched_report(args, count=64, seed=20261204):
+    """64 independent H2-b matrices: N log-uniform in [4096, 65536], d from {8, 18, 28, 54},
+    Gaussian kernel (h uniform in [0.5, 3]) or inverse multiquadric 1/sqrt(1 + r^2/h^2), nrhs
+    log-uniform in [32, 512], W drawn in FP32 from N(0, 1); leaf 256, budget 0.03, ID tolerance
+    1e-5, max rank 256; points from a 16-component mixture (means uniform in [-2, 2]^d, sigma
+    uniform in [0.3, 1.0]).  Split-BF16 plans evaluated as one batch (one graph, autotuned
+    tiles) and one by one; every result checked against an FP64 plan of the same CDS."""
+    import torch
+    from matrox_ru_b200 import build as mbuild, hgemm as H, structure as S
+    mbuild.build()
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(seed)
+    plans, TWs, refs, nrhs, shapes = [], [], [], [], []
+    flops, t_build = 0, time.time()
+    for i in range(count):
+        n = int(np.exp(rng.uniform(np.log(4096), np.log(65536))))
+        d = int(rng.choice([8, 18, 28, 54]))
+        kind = "gaussian" if rng.uniform() < 0.5 else "imq"
+        h = float(rng.uniform(0.5, 3.0))
+        r = int(np.exp(rng.uniform(np.log(32), np.log(512))))
+        X = S.gaussian_mixture(n, d, 16, -2.0, 2.0, 0.3, 1.0, seed=seed + i)
+        cds = S.build_cds(X, S.KernelSpec(kind, h), leaf_size=256, budget=0.03, tol=1e-5, max_rank=256,
+                          seed=seed + i)
+        g = torch.Generator(device=dev).manual_seed(seed + i)
+        TW = torch.randn(cds.n * r, dtype=torch.float32, device=dev, generator=g).double()
+        p64 = H.Plan(cds, "fp64")
+        refs.append(p64.evaluate(TW, r))
+        del p64
+        plans.append(H.Plan(cds, "split_bf16"))
+        plans[-1].cds = None  # the plan holds its own device copy; free the host CDS
+        TWs.append(TW)
+        nrhs.append(r)
+        flops += cds.flops(r)
+        shapes.append([cds.n, d, kind, round(h, 2), r])
+        del cds, X
+    t_build = time.time() - t_build
+    torch.cuda.synchronize()
+
+    def timed(fn, steps):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        e1.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    batch = H.Batch(plans)
+    outs = [torch.zeros_like(t) for t in TWs]
+    batch_ms = timed(lambda: batch.evaluate(TWs, nrhs, outs=outs), args.steps)
+    batch.status()
+    errs = [float(torch.linalg.norm(o - y) / torch.linalg.norm(y)) for o, y in zip(outs, refs)]
+    single_ms = 0.0
+    for p, t, r, o in zip(plans, TWs, nrhs, outs):
+        single_ms += timed(lambda p=p, t=t, r=r, o=o: p.evaluate(t, r, out=o), args.steps)
+        p.status()
+    info = batch.info()
+    line = {"report": "batched uneven H2-b matrices", "matrices": count, "algorithmic_flops": flops,
+            "batch_ms": round(batch_ms, 3), "sum_of_single_plan_ms": round(single_ms, 3),
+            "batch_tflops": round(flops / (batch_ms * 1e-3) / 1e12, 2),
+            "launches_per_batch_evaluation": info["launches"],
+            "launches_single_plans": sum(p.info()["launches"] for p in plans),
+            "tuned_tiles": {"widths": info["widths"], "pairs": info["pairs"]},
+            "max_rel_err_vs_fp64_same_cds": max(errs), "median_rel_err": float(np.median(errs)),
+            "rel_err_per_matrix": [float(f"{e:.3g}") for e in errs],
+            "cds_build_s": round(t_build, 1), "matrices_n_d_kernel_h_nrhs": shapes}
+    print(json.dumps(line), flush=True)
 
 
 def tolerance_sweep(args, cfg):
@@ -258,6 +333,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.tolerance_sweep:
         tolerance_sweep(args, cfg)
+        return
+    if args.batched:
+        batched_report(args)
         return
     if args.impl == "reference":
         if world > 1:
