@@ -183,6 +183,11 @@ def build_cds(cfg):
     return X, cds, time.time() - t
 
 
+def S_kernel_spec(cfg):
+    from matrox_ru_b200 import structure as S
+    return S.KernelSpec(cfg["kernel"], cfg["h"])
+
+
 def leaf_slice(cds, TW, r_full, r):
     """First r columns of every leaf block of a packed leaf-blocked array (r_full columns)."""
     out = np.empty(cds.n * r)
@@ -364,6 +369,28 @@ def main():
     r = cfg["nrhs"]
     flops = cds.flops(r)
     fb = cds.flops_breakdown(r)
+    # the near blocks and far couplings generated on the device from the points (the reference
+    # assembles them on the host), against the host assembly used below
+    gpu_blocks = None
+    if rank == 0:
+        spec = S_kernel_spec(cfg)
+        H.kernel_blocks(cds, X, spec)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        dD, dB = H.kernel_blocks(cds, X, spec)
+        e1.record()
+        e1.synchronize()
+        bms = e0.elapsed_time(e1)
+        diff = 0.0
+        for dv, hv in ((dD, cds.D), (dB, cds.B)):
+            ht = torch.as_tensor(hv, device=dev)
+            diff = max(diff, ((dv[:ht.numel()] - ht).abs().max() / ht.abs().max()).item())
+            del ht
+        nbytes = (cds.D.size + cds.B.size) * 8
+        gpu_blocks = {"ms": round(bms, 3), "bytes": nbytes, "tb_per_s": round(nbytes / (bms * 1e-3) / 1e12, 2),
+                      "max_rel_diff_vs_host_assembly": diff}
+        del dD, dB
+        torch.cuda.empty_cache()
     # tensor-core flops each split mode executes: 3 or 6 bf16 products per algorithmic product
     exec_flops = {"fp64": flops,
                   "split_bf16": 3 * (fb["near"] + fb["far"]) + 6 * fb["tree"],
@@ -571,7 +598,7 @@ def main():
         "gflops": round(flops / (ms * 1e-3) / 1e9, 1),
         "aggregate_gflops": round(world * flops / (ms * 1e-3) / 1e9, 1),
         "modes": results, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-        "clocks": clocks, "cds_build_s": round(t_build, 1),
+        "clocks": clocks, "cds_build_s": round(t_build, 1), "gpu_cds_blocks": gpu_blocks,
     }
     if rank == 0:
         print(json.dumps(line))

@@ -201,7 +201,9 @@ typedef struct mxb_cds_desc {
     const int32_t *fpairx, *fpairy; int32_t fcount;
 } mxb_cds_desc;
 
-/* Uploads and repacks the CDS for `precision`, builds the task lists; device = current. */
+/* Uploads and repacks the CDS for `precision`, builds the task lists; device = current.
+ * desc->D, desc->B and desc->VT may be host arrays or device arrays of the current device
+ * (e.g. blocks from mxb_kernel_blocks); the plan keeps its own copy either way. */
 MXB_API int32_t mxb_plan_create(const mxb_cds_desc *desc, int32_t precision, mxb_plan **out);
 MXB_API int32_t mxb_plan_destroy(mxb_plan *plan);
 /* dY (+)= K~ dW on `stream` (a cudaStream_t, 0 = legacy default).  dW / dY are device
@@ -291,6 +293,26 @@ MXB_API int32_t mxb_plan_profile(mxb_plan *plan, const double *dW, double *dY, i
 MXB_API int32_t mxb_batch_profile(mxb_batch *batch, const double *const *dW, double *const *dY,
                                   const int32_t *nrhs, void *stream, mxb_op_profile *out, int32_t cap,
                                   int32_t *nops);
+
+/* ---- CDS blocks generated on the GPU ---------------------------------------------------- */
+
+/* Replaces the host-side block assembly of the CDS: Fsubmatrix, matroxTest-V1/compression.h:
+ * 256-360, packed by CacheNear / CacheFar, matroxTest-V1/hcds.h:339-460.  Computes kernel blocks
+ * K(X[rows], X[cols]) on the device, each stored column-major (element (i, j) at
+ * out + blk_ofs[b] + i + j * rows) as in the reference's D / B pools.  dX: device points,
+ * n x d row-major FP64 (d <= 128).  Index sets: host CSR, set s = set_idx[set_ofs[s] ..
+ * set_ofs[s + 1]) (point indices; leaf points for near blocks, skeleton points for far
+ * couplings).  Block b has rows from set blk_row[b] and columns from set blk_col[b].  dOut:
+ * device array of out_len elements.  kind: MXB_KERNEL_*; h: bandwidth (unused for
+ * MXB_KERNEL_NEWTON).  Asynchronous on `stream`; allocates its tile list with
+ * cudaMallocAsync. */
+#define MXB_KERNEL_GAUSSIAN 0 /* exp(-|x-y|^2 / (2 h^2))                               */
+#define MXB_KERNEL_IMQ 1      /* 1 / sqrt(1 + |x-y|^2 / h^2)                            */
+#define MXB_KERNEL_NEWTON 2   /* 1 / |x-y|, 1 on coincident points (compression.h:338)  */
+MXB_API int32_t mxb_kernel_blocks(const double *dX, int64_t n, int32_t d, int32_t kind, double h,
+                                  const int64_t *set_ofs, const int32_t *set_idx, int32_t nsets,
+                                  const int32_t *blk_row, const int32_t *blk_col, const uint64_t *blk_ofs,
+                                  int32_t nblk, double *dOut, uint64_t out_len, void *stream);
 
 /* ---- evaluation without device allocation ------------------------------------------------ */
 

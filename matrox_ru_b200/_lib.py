@@ -27,6 +27,7 @@ FLAG_MIRROR_WORKSPACES = 1
 FLAG_OUTPUT_IS_ZERO = 2
 DEBUG_STALL_ONE_WAIT = 1
 TILE_PAIR = 4096
+KERNEL_KINDS = {"gaussian": 0, "imq": 1, "newton": 2}
 PHASES = {0: "split_w", 1: "up", 2: "far", 3: "down", 4: "near", 5: "leaf_down", 6: "far_down",
           7: "near_leaf_down", 8: "far_near"}
 
@@ -109,6 +110,7 @@ def load(path: str = LIB_PATH):
     lib.mxb_transform.argtypes = [P, P, P, I32, P, I64, I64, I32, P]
     lib.mxb_untransform.argtypes = [P, P, P, I32, P, I64, I64, I32, P]
     lib.mxb_evaluate_noalloc.argtypes = [ctypes.POINTER(CdsDesc), P, P, I32, I32, P]
+    lib.mxb_kernel_blocks.argtypes = [P, I64, I32, I32, ctypes.c_double, P, P, I32, P, P, P, I32, P, U64, P]
     lib.mxb_hgemm_set_shape.argtypes = [I32, I32, I32]
     lib.mxb_hgemm_hss_set_shape.argtypes = [I32, I32]
     cb = _REF_ARGS_H2B + [I32, I32, P, P, ctypes.c_int]

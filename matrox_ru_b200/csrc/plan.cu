@@ -383,16 +383,16 @@ int Plan::create(const mxb_cds_desc &d, int prec, Plan **out)
     int rc = p->validate(d);
     if (rc) return rc;
     p->build_tasks(row_tile_for(prec));
-    // FP64 CDS
+    // FP64 CDS (host or device arrays: cudaMemcpyDefault follows the pointers)
     rc = p->alloc((void **)&p->dD, std::max<uint64_t>(d.D_len, 1) * sizeof(double));
     if (rc) return rc;
-    MXB_CUDA(cudaMemcpy(p->dD, d.D, d.D_len * sizeof(double), cudaMemcpyHostToDevice));
+    MXB_CUDA(cudaMemcpy(p->dD, d.D, d.D_len * sizeof(double), cudaMemcpyDefault));
     rc = p->alloc((void **)&p->dB, std::max<uint64_t>(d.B_len, 1) * sizeof(double));
     if (rc) return rc;
-    if (d.B_len) MXB_CUDA(cudaMemcpy(p->dB, d.B, d.B_len * sizeof(double), cudaMemcpyHostToDevice));
+    if (d.B_len) MXB_CUDA(cudaMemcpy(p->dB, d.B, d.B_len * sizeof(double), cudaMemcpyDefault));
     rc = p->alloc((void **)&p->dVT, std::max<uint64_t>(d.VT_len, 1) * sizeof(double));
     if (rc) return rc;
-    if (d.VT_len) MXB_CUDA(cudaMemcpy(p->dVT, d.VT, d.VT_len * sizeof(double), cudaMemcpyHostToDevice));
+    if (d.VT_len) MXB_CUDA(cudaMemcpy(p->dVT, d.VT, d.VT_len * sizeof(double), cudaMemcpyDefault));
     rc = p->alloc((void **)&p->dTasks, p->tasks.size() * sizeof(Task));
     if (rc) return rc;
     if (!p->tasks.empty())

@@ -197,16 +197,59 @@ def _profile_records(recs, n):
              "pair": bool(r.pair), "flops": r.flops, "issued_flops": r.issued_flops, "ms": r.ms} for r in recs[:min(n, len(recs))]]
 
 
-class Plan:
-    """Device-resident CDS and task lists (``mxb_plan_*``)."""
+def kernel_blocks(cds, X, kernel, stream=None):
+    """The CDS's near blocks D and far couplings B computed on the GPU from the points
+    (``mxb_kernel_blocks``; the reference computes them on the host with ``Fsubmatrix``,
+    ``matroxTest-V1/compression.h:256-360``).  X: (N, d) float64 points, host or CUDA;
+    kernel: a :class:`~matrox_ru_b200.structure.KernelSpec`.  Returns CUDA tensors (D, B) in the
+    layout of ``cds.D`` / ``cds.B`` (offsets ``cds.Dptr`` / ``cds.Bptr``)."""
+    torch = _torch()
+    dX = torch.as_tensor(np.ascontiguousarray(X, dtype=np.float64)).to("cuda")
+    n, d = dX.shape
+    # index sets: the points of every leaf (tree order), then the skeleton points of every node
+    leaf_sets = [cds.perm[int(cds.leaf_lids_offset[i]):int(cds.leaf_lids_offset[i + 1])] for i in range(cds.nleaf)]
+    skel_sets = [np.asarray(s if s is not None else [], dtype=np.int64) for s in cds.skels]
+    sets = leaf_sets + skel_sets
+    set_ofs = np.concatenate([[0], np.cumsum([len(s) for s in sets])]).astype(np.int64)
+    set_idx = np.concatenate(sets).astype(np.int32) if len(set_ofs) > 1 and set_ofs[-1] else np.zeros(1, np.int32)
+    nl = cds.nleaf
+    # the near pair list holds leaf indices; far pairs hold node indices
+    out = []
+    for rows, cols, ofs, length in ((np.asarray(cds.npairx), np.asarray(cds.npairy), cds.Dptr, cds.D.size),
+                                    (np.asarray(cds.fpairx) + nl, np.asarray(cds.fpairy) + nl, cds.Bptr, cds.B.size)):
+        dst = torch.empty(max(int(length), 1), dtype=torch.float64, device=dX.device)
+        a = _Args()
+        check(_lib.load().mxb_kernel_blocks(dX.data_ptr(), n, d, _lib.KERNEL_KINDS[kernel.kind], float(kernel.h),
+                                            a(set_ofs, np.int64), a(set_idx), len(sets), a(rows), a(cols),
+                                            a(ofs, np.uint64), len(rows), dst.data_ptr(), int(length),
+                                            _stream_ptr(stream)), "mxb_kernel_blocks")
+        out.append(dst)
+    return out[0], out[1]
 
-    def __init__(self, cds, precision: str = "fp64"):
+
+class Plan:
+    """Device-resident CDS and task lists (``mxb_plan_*``).  ``pools`` optionally gives the
+    numeric pools (D, B, VT) as CUDA tensors (e.g. from :func:`kernel_blocks`) instead of the
+    CDS's host arrays."""
+
+    def __init__(self, cds, precision: str = "fp64", pools=None):
         torch = _torch()
         if not torch.cuda.is_available():
             raise RuntimeError("matrox_ru_b200.Plan needs a CUDA device")
         lib = _lib.load()
         keep: list = []
         desc = cds_desc(cds, keep)
+        if pools is not None:
+            for name, t in zip(("D", "B", "VT"), pools):
+                if t is None:
+                    continue
+                if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
+                    raise TypeError("device pools must be contiguous float64 CUDA tensors")
+                if t.numel() < getattr(cds, name).size:
+                    raise ValueError(f"device pool {name} is smaller than the CDS's")
+                keep.append(t)
+                setattr(desc, name, t.data_ptr())
+            torch.cuda.synchronize()  # the pools were written on torch's stream
         h = P()
         check(lib.mxb_plan_create(ctypes.byref(desc), PRECISIONS[precision], ctypes.byref(h)), "mxb_plan_create")
         self._h = h

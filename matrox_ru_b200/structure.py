@@ -77,15 +77,25 @@ def sqdist(A: np.ndarray, B: np.ndarray) -> np.ndarray:
 
 
 def kernel_matrix(X: np.ndarray, rows, cols, spec: KernelSpec) -> np.ndarray:
-    """Dense kernel block K(X[rows], X[cols]) in FP64 (C-ordered, rows x cols)."""
+    """Dense kernel block K(X[rows], X[cols]) in FP64 (C-ordered, rows x cols).
+
+    The Gaussian and the inverse multiquadric take squared distances from the norm expansion
+    (as the reference's Gaussian does, ``compression.h:256-300``).  The 1/r kernel sums the
+    squared coordinate differences, as the reference does (``compression.h:338-350``), so
+    coincident points give exactly 0 and the value 1."""
+    if spec.kind == "newton":
+        A, B = X[rows], X[cols]
+        d2 = np.zeros((len(A), len(B)))
+        for k in range(X.shape[1]):
+            diff = A[:, k][:, None] - B[:, k][None, :]
+            d2 += diff * diff
+        r = np.sqrt(d2)
+        r[r == 0] = 1.0
+        return 1.0 / r
     d2 = sqdist(X[rows], X[cols])
     if spec.kind == "gaussian":
         return np.exp(d2 * (-0.5 / (spec.h * spec.h)))
-    if spec.kind == "imq":
-        return 1.0 / np.sqrt(1.0 + d2 / (spec.h * spec.h))
-    r = np.sqrt(d2)
-    r[r == 0] = 1.0
-    return 1.0 / r
+    return 1.0 / np.sqrt(1.0 + d2 / (spec.h * spec.h))
 
 
 # ---------------------------------------------------------------------------
