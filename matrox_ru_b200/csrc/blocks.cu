@@ -7,8 +7,9 @@
 // by CacheNear / CacheFar (matroxTest-V1/hcds.h:339-460).  Here one kernel fills any list of
 // such blocks: a CTA computes a 64 x 64 tile of one block from the tile's row and column
 // points staged in shared memory, squared distances summed coordinate by coordinate in FP64,
-// then the kernel function.  The output writes are coalesced along the block's rows; the work
-// is bound by those writes (8 bytes per element) for the dimensions the reference targets.
+// then the kernel function.  The output writes are coalesced along the block's rows.  At
+// d = 28 the work is bound by the FP64 arithmetic (d FMAs and one exp per element), not by the
+// writes (8 bytes per element).
 #include <algorithm>
 #include <string>
 #include <vector>
@@ -54,24 +55,39 @@ __global__ void __launch_bounds__(THREADS) kernel_block_kernel(const BlockTile *
         Q[p * ld + k] = p < nc ? X[(int64_t)idx[t.cols0 + t.c0 + p] * d + k] : 0.0;
     }
     __syncthreads();
-    // thread: one row i, 16 columns j0 .. j0 + 15
-    const int i = threadIdx.x & (TILE - 1), j0 = (threadIdx.x >> 6) * 16;
-    double d2[16];
+    // thread (tr, tc): rows tr + 16 a and columns tc + 16 b (a, b < 4), a 4 x 4 register
+    // block: 8 shared-memory loads per coordinate for 16 FMAs; the writes of 16 consecutive
+    // threads cover 16 consecutive rows of a column
+    const int tr = threadIdx.x & 15, tc = threadIdx.x >> 4;
+    double d2[4][4];
 #pragma unroll
-    for (int q = 0; q < 16; ++q) d2[q] = 0.0;
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) d2[a][b] = 0.0;
     for (int k = 0; k < d; ++k) {
-        const double a = P[i * ld + k];
+        double pa[4], qb[4];
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-            const double diff = a - Q[(j0 + q) * ld + k];
-            d2[q] = fma(diff, diff, d2[q]);
-        }
+        for (int a = 0; a < 4; ++a) pa[a] = P[(tr + 16 * a) * ld + k];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) qb[b] = Q[(tc + 16 * b) * ld + k];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const double diff = pa[a] - qb[b];
+                d2[a][b] = fma(diff, diff, d2[a][b]);
+            }
     }
-    if (i < nr) {
-        double *o = out + t.out + (uint64_t)(t.r0 + i) + (uint64_t)(t.c0 + j0) * (uint64_t)t.nrows;
+    double *o = out + t.out + (uint64_t)t.r0 + (uint64_t)t.c0 * (uint64_t)t.nrows;
 #pragma unroll
-        for (int q = 0; q < 16; ++q)
-            if (j0 + q < nc) o[(uint64_t)q * t.nrows] = kernel_value(d2[q], kind, s);
+    for (int b = 0; b < 4; ++b) {
+        const int j = tc + 16 * b;
+        if (j >= nc) continue;
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const int i = tr + 16 * a;
+            if (i < nr) o[(uint64_t)i + (uint64_t)j * t.nrows] = kernel_value(d2[a][b], kind, s);
+        }
     }
 }
 
