@@ -405,7 +405,7 @@ def main():
     modes = ["fp64", "split_bf16", "split_bf16_far6", "split_bf16_x6"] if args.precision == "all" \
         else [args.precision]
     results = {}
-    outs = {}  # host copy of every mode's result, to check the drop-in's output against
+    outs = {}  # first 16 columns of every mode's result, to check the drop-in's output against
     clocks = None
     stream = torch.cuda.current_stream()
     for mode in modes:
@@ -479,7 +479,7 @@ def main():
             Yo = cds.from_tree_order(Ys, rc)[rows]
             res["rel_err_vs_dense_64rows"] = float(np.linalg.norm(Yo - Yd) / np.linalg.norm(Yd))
         results[mode] = res
-        outs[mode] = out.cpu().numpy()
+        outs[mode] = leaf_slice(cds, out.cpu().numpy(), r, 16)
         if clocks is None:
             clocks = res["clocks"]
         del plan, out
@@ -519,6 +519,8 @@ def main():
     # end to end through the reference-signature drop-in, host buffers (pinned)
     e2e = None
     out_keep = outs.get(best)
+    import gc
+    gc.collect()
     if not args.no_e2e:
         H.set_precision(best)
         pin_tw = torch.empty(cds.n * r, dtype=torch.float64, pin_memory=True)
@@ -551,7 +553,8 @@ def main():
         nb = cds.n * r * 8
         e2e_ms = timed_dropin(_lib.FLAG_OUTPUT_IS_ZERO)
         # parity of the timed drop-in output with the device-timed evaluation
-        e2e_err = float(np.abs(y_np - out_keep).max() / np.abs(out_keep).max()) if out_keep is not None else None
+        ys = leaf_slice(cds, y_np, r, 16)
+        e2e_err = float(np.abs(ys - out_keep).max() / np.abs(out_keep).max()) if out_keep is not None else None
         acc_ms = timed_dropin(0)
         H.set_flags(0)
         e2e = {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": nb, "d2h_bytes_per_step": nb,
