@@ -124,6 +124,42 @@ def batched_report(args, count=64, seed=20261204):
     print(json.dumps(line), flush=True)
 
 
+def caller_order_timing(torch, H, plan, cds, TW, r, steps):
+    """W and Y as row-major (N, r) arrays in the caller's point order: the fused evaluation
+    (rows gathered while W is split into operand tiles, scattered by the epilogues that write
+    Y) against the unfused sequence permute -> leaf-blocked evaluation -> permute.  Device time
+    with CUDA events, inputs larger than L2; the two results are compared."""
+    ev = H.Evaluator(cds, plan=plan)
+    W = ev.from_tree(TW, r)  # the benchmark's W in the caller's order
+    Y = torch.empty_like(W)
+    TY = torch.empty_like(TW)
+
+    def fused():
+        plan.evaluate_ordered(W, out=Y)
+
+    def unfused():
+        ev.from_tree(plan.evaluate(ev.to_tree(W), r, out=TY), r, out=Yu)
+
+    Yu = torch.empty_like(W)
+    out = {}
+    for name, fn in (("fused_ms", fused), ("unfused_ms", unfused)):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        e1.synchronize()
+        out[name] = round(e0.elapsed_time(e1) / steps, 4)
+    plan.status()
+    out["max_rel_diff_fused_vs_unfused"] = float((Y - Yu).abs().max() / Yu.abs().max())
+    out["layout"] = "W, Y row-major (N, r) in the caller's point order"
+    del W, Y, Yu, TY
+    return out
+
+
 def tolerance_sweep(args, cfg):
     """Relative error of the FP64 and split-BF16 evaluators against the dense FP64 K W (64
     sampled rows) and of split-BF16 against FP64 on the same CDS, at three ID tolerances."""
@@ -478,6 +514,8 @@ def main():
             Yd = S.dense_kernel_times(X, Wo, S.KernelSpec(cfg["kernel"], cfg["h"]), rows=rows)
             Yo = cds.from_tree_order(Ys, rc)[rows]
             res["rel_err_vs_dense_64rows"] = float(np.linalg.norm(Yo - Yd) / np.linalg.norm(Yd))
+        if mode == "split_bf16":
+            res["caller_order"] = caller_order_timing(torch, H, plan, cds, TW, r, args.steps)
         results[mode] = res
         outs[mode] = leaf_slice(cds, out.cpu().numpy(), r, 16)
         if clocks is None:

@@ -217,6 +217,24 @@ MXB_API int32_t mxb_plan_evaluate(mxb_plan *plan, const double *dW, double *dY, 
 MXB_API int32_t mxb_plan_adjoint(mxb_plan *plan, const double *dG, double *dGW, int32_t nrhs,
                          const int32_t *gptr, const int32_t *gwptr, int32_t accumulate,
                          void *stream);
+/* W and Y in the caller's point order.  The reference permutes W into tree order before
+ * HGEMM (`transform`, matroxTest-V1/hcds.h:766-788, called from matroxTest-V1/main.cpp:91) and
+ * leaves Y in tree order (matroxTest-V1/Util.h:320).  Here the permutation is registered once:
+ * perm[t] is the caller's row of tree position t (the reference's `lids`; host or device
+ * array of sum(Ddim) entries, checked to be a permutation).  Synchronous. */
+MXB_API int32_t mxb_plan_set_permutation(mxb_plan *plan, const int32_t *perm);
+/* dY (+)= K~ dW with dW / dY in the caller's point order: element (p, j) of dW at
+ * dW[p * w_rs + j * w_cs] (row-major (N, nrhs): w_rs = nrhs, w_cs = 1; column-major: 1, ld),
+ * likewise dY.  Split-BF16 plans gather W's rows inside the launch that splits W into operand
+ * tiles and scatter Y's rows in the epilogues that write Y, so the permutation costs no pass of
+ * its own; FP64 plans permute into leaf-blocked copies and back.  Asynchronous. */
+MXB_API int32_t mxb_plan_evaluate_ordered(mxb_plan *plan, const double *dW, int64_t w_rs, int64_t w_cs,
+                                          double *dY, int64_t y_rs, int64_t y_cs, int32_t nrhs,
+                                          int32_t accumulate, void *stream);
+/* dGW (+)= K~^T dG in the caller's point order (FP64 plans; permuted copies). */
+MXB_API int32_t mxb_plan_adjoint_ordered(mxb_plan *plan, const double *dG, int64_t g_rs, int64_t g_cs,
+                                         double *dGW, int64_t gw_rs, int64_t gw_cs, int32_t nrhs,
+                                         int32_t accumulate, void *stream);
 /* Algorithmic flops of one evaluation (matroxTest-V1/compression.h:1079-1130). */
 MXB_API int32_t mxb_plan_flops(const mxb_plan *plan, int32_t nrhs, uint64_t *flops);
 /* Bytes of CDS held on the device and number of kernel launches of one evaluation. */

@@ -93,6 +93,9 @@ def load(path: str = LIB_PATH):
     lib.mxb_plan_destroy.argtypes = [P]
     lib.mxb_plan_evaluate.argtypes = [P, P, P, I32, P, P, I32, P]
     lib.mxb_plan_adjoint.argtypes = [P, P, P, I32, P, P, I32, P]
+    lib.mxb_plan_set_permutation.argtypes = [P, P]
+    lib.mxb_plan_evaluate_ordered.argtypes = [P, P, I64, I64, P, I64, I64, I32, I32, P]
+    lib.mxb_plan_adjoint_ordered.argtypes = [P, P, I64, I64, P, I64, I64, I32, I32, P]
     lib.mxb_plan_flops.argtypes = [P, I32, ctypes.POINTER(U64)]
     lib.mxb_plan_info.argtypes = [P, ctypes.POINTER(U64), ctypes.POINTER(I32), ctypes.POINTER(I32)]
     lib.mxb_plan_read_workspaces.argtypes = [P, I32, P, P, P, P]

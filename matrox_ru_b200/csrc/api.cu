@@ -12,12 +12,6 @@
 #include "mxb_internal.h"
 #include "plan.h"
 
-namespace mxb {
-cudaError_t launch_permute(const int32_t *perm, const int32_t *leafofs, const int32_t *blockofs, int nleaf,
-                           int64_t n, const double *src, double *dst, int64_t rs, int64_t cs, int nrhs,
-                           int dir, int accumulate, cudaStream_t stream);
-}
-
 using namespace mxb;
 
 #define API_CUDA(call)                                                                    \
@@ -838,6 +832,37 @@ int32_t mxb_plan_adjoint(mxb_plan *plan, const double *dG, double *dGW, int32_t 
     }
     Plan *p = static_cast<Plan *>(plan);
     return p->run(p->launches_adj, dG, dGW, nrhs, gptr, gwptr, accumulate, (cudaStream_t)stream);
+}
+
+int32_t mxb_plan_set_permutation(mxb_plan *plan, const int32_t *perm)
+{
+    if (!plan) {
+        set_error("null plan");
+        return MXB_ERR_ARG;
+    }
+    return static_cast<Plan *>(plan)->set_permutation(perm);
+}
+
+int32_t mxb_plan_evaluate_ordered(mxb_plan *plan, const double *dW, int64_t w_rs, int64_t w_cs, double *dY,
+                                  int64_t y_rs, int64_t y_cs, int32_t nrhs, int32_t accumulate, void *stream)
+{
+    if (!plan) {
+        set_error("null plan");
+        return MXB_ERR_ARG;
+    }
+    return static_cast<Plan *>(plan)->run_ordered(false, dW, w_rs, w_cs, dY, y_rs, y_cs, nrhs, accumulate,
+                                                  (cudaStream_t)stream);
+}
+
+int32_t mxb_plan_adjoint_ordered(mxb_plan *plan, const double *dG, int64_t g_rs, int64_t g_cs, double *dGW,
+                                 int64_t gw_rs, int64_t gw_cs, int32_t nrhs, int32_t accumulate, void *stream)
+{
+    if (!plan) {
+        set_error("null plan");
+        return MXB_ERR_ARG;
+    }
+    return static_cast<Plan *>(plan)->run_ordered(true, dG, g_rs, g_cs, dGW, gw_rs, gw_cs, nrhs, accumulate,
+                                                  (cudaStream_t)stream);
 }
 
 int32_t mxb_plan_flops(const mxb_plan *plan, int32_t nrhs, uint64_t *flops)

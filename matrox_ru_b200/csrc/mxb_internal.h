@@ -73,6 +73,22 @@ cudaError_t launch_gemm_f64(const Task *tasks, const Item *items, int ntasks,
 
 cudaError_t prepare_gemm_f64();  // sets the kernel's shared-memory limit (before any capture)
 
+// Row permutation between the caller's point order and the leaf-blocked tree order
+// (permute.cu): dir 0 gathers dst(leaf-blocked) = src[perm rows], dir 1 scatters
+// dst[perm rows] (+)= src(leaf-blocked).  The caller-order matrix has element (p, j) at
+// p * rs + j * cs; leafofs has nleaf + 1 entries, blockofs nleaf.
+cudaError_t launch_permute(const int32_t *perm, const int32_t *leafofs, const int32_t *blockofs, int nleaf,
+                           int64_t n, const double *src, double *dst, int64_t rs, int64_t cs, int nrhs,
+                           int dir, int accumulate, cudaStream_t stream);
+
+// W and Y of an evaluation in the caller's point order: tree position t of leaf i (t in
+// [tofs[i], tofs[i + 1])) is row perm[t]; element (row, j) sits at row * rs + j * cs.
+struct CallerOrder {
+    const int32_t *perm;
+    const int32_t *tofs;
+    int64_t w_rs, w_cs, y_rs, y_cs;
+};
+
 void set_error(const std::string &msg);
 
 }  // namespace mxb

@@ -75,6 +75,12 @@ static int fail(const std::string &m)
     return MXB_ERR_STRUCTURE;
 }
 
+static int arg_fail(const std::string &m)
+{
+    set_error(m);
+    return MXB_ERR_ARG;
+}
+
 int Plan::validate(const mxb_cds_desc &d)
 {
     if (d.nleaf < 1 || d.numnodes < 1 || d.ncount < 0 || d.fcount < 0) {
@@ -532,6 +538,81 @@ int Plan::run(const std::vector<Launch> &L, const double *dW, double *dY, int nr
         hit = &graphs.back();
     }
     MXB_CUDA(cudaGraphLaunch(hit->exec, stream));
+    return MXB_OK;
+}
+
+// The caller's point order: perm[t] is the row of W / Y holding tree position t (the `lids`
+// order of matroxTest-V1/hcds.h:766-788).  Host or device array; checked to be a permutation.
+int Plan::set_permutation(const int32_t *perm)
+{
+    if (!perm) return arg_fail("null permutation");
+    const int64_t n = rows_total;
+    std::vector<int32_t> h((size_t)n + nleaf + 1);
+    MXB_CUDA(cudaMemcpy(h.data(), perm, sizeof(int32_t) * (size_t)n, cudaMemcpyDefault));
+    std::vector<char> seen((size_t)n, 0);
+    for (int64_t t = 0; t < n; ++t) {
+        const int32_t q = h[(size_t)t];
+        if (q < 0 || q >= n || seen[(size_t)q]) return arg_fail("perm is not a permutation of the plan's rows");
+        seen[(size_t)q] = 1;
+    }
+    for (int i = 0; i <= nleaf; ++i) h[(size_t)n + i] = (int32_t)(i < nleaf ? leaf_row[i] : n);
+    if (!dTree) {
+        int rc = alloc((void **)&dTree, h.size() * sizeof(int32_t));
+        if (rc) return rc;
+    }
+    MXB_CUDA(cudaMemcpy(dTree, h.data(), h.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    MXB_CUDA(cudaDeviceSynchronize());  // a pageable upload may return before it lands
+    return MXB_OK;
+}
+
+// dY (+)= K~ dW (or K~^T) with dW / dY in the caller's point order.  Split-BF16 forward
+// evaluations gather W's rows inside the launch that splits W into operand tiles and scatter
+// Y's rows in the epilogues that write Y: no extra pass over either matrix.  Other paths
+// (FP64, the adjoint) permute into leaf-blocked copies, evaluate, and permute back.
+int Plan::run_ordered(bool adjoint, const double *dW, int64_t w_rs, int64_t w_cs, double *dY, int64_t y_rs,
+                      int64_t y_cs, int nrhs, int accumulate, cudaStream_t stream)
+{
+    if (!dTree) return arg_fail("no point order set (mxb_plan_set_permutation)");
+    if (!dW || !dY || nrhs < 1) return arg_fail("bad caller-order operands");
+    const int64_t n = rows_total;
+    // distinct elements must not alias: one stride has to step over the whole other extent
+    auto separated = [&](int64_t rs, int64_t cs) {
+        return rs >= 1 && cs >= 1 && (rs >= (int64_t)nrhs * cs || cs >= n * rs);
+    };
+    if (!separated(w_rs, w_cs) || !separated(y_rs, y_cs)) return arg_fail("caller-order strides overlap");
+    const std::vector<Launch> &L = adjoint ? launches_adj : launches_fwd;
+    if (precision != MXB_PREC_FP64 && !adjoint) {
+        int cur = -1;
+        MXB_CUDA(cudaGetDevice(&cur));
+        if (cur != device) return arg_fail("plan used on a different device than it was created on");
+        int rc = stage_offsets(0, nullptr, nrhs, stream);
+        if (!rc) rc = stage_offsets(1, nullptr, nrhs, stream);
+        if (rc) return rc;
+        const CallerOrder o{dTree, dTree + n, w_rs, w_cs, y_rs, y_cs};
+        return run_split_bf16(L, dW, dY, nrhs, accumulate, stream, &o);
+    }
+    const size_t need = (size_t)std::max<int64_t>(n, 1) * nrhs;
+    if (need > order_elems) {
+        for (double **q : {&dTW, &dTY}) {
+            if (!*q) continue;
+            cudaFree(*q);
+            allocations.erase(std::remove(allocations.begin(), allocations.end(), (void *)*q), allocations.end());
+            *q = nullptr;
+        }
+        device_bytes -= 2 * order_elems * sizeof(double);
+        order_elems = 0;
+        int rc = alloc((void **)&dTW, need * sizeof(double));
+        if (!rc) rc = alloc((void **)&dTY, need * sizeof(double));
+        if (rc) return rc;
+        order_elems = need;
+    }
+    int rc = stage_offsets(0, nullptr, nrhs, stream);  // packed blocks of the leaf-blocked copies
+    if (rc) return rc;
+    MXB_CUDA(launch_permute(dTree, dTree + n, dOfs, nleaf, n, dW, dTW, w_rs, w_cs, nrhs, 0, 0, stream));
+    rc = run(L, dTW, dTY, nrhs, nullptr, nullptr, 0, stream);
+    if (rc) return rc;
+    MXB_CUDA(launch_permute(dTree, dTree + n, dOfs + nleaf, nleaf, n, dTY, dY, y_rs, y_cs, nrhs, 1, accumulate,
+                            stream));
     return MXB_OK;
 }
 

@@ -46,6 +46,11 @@ struct Plan : public mxb_plan {
     std::vector<int32_t> ofs_host[4];
     double *dWskel = nullptr, *dUskel = nullptr;
     size_t scratch_elems = 0;
+    // caller point order (mxb_plan_set_permutation): perm (rows_total entries) followed by
+    // the first tree position of every leaf (nleaf + 1 entries)
+    int32_t *dTree = nullptr;
+    double *dTW = nullptr, *dTY = nullptr;  // leaf-blocked copies for the unfused caller-order path
+    size_t order_elems = 0;
     SplitBF16 *bf16 = nullptr;
     int debug_flags = 0;              // test hooks (mxb_plan_set_test_hooks)
     long long debug_wait_cycles = 0;  // 0: default wait limit
@@ -64,6 +69,9 @@ struct Plan : public mxb_plan {
             const int32_t *yofs, int accumulate, cudaStream_t stream);
     int profile(const double *dW, double *dY, int nrhs, cudaStream_t stream, mxb_op_profile *out, int cap,
                 int *nops);
+    int set_permutation(const int32_t *perm);
+    int run_ordered(bool adjoint, const double *dW, int64_t w_rs, int64_t w_cs, double *dY, int64_t y_rs,
+                    int64_t y_cs, int nrhs, int accumulate, cudaStream_t stream);
     int read_workspaces(int nrhs, const int32_t *wsko, double *wskel, const int32_t *usko, double *uskel);
     uint64_t flops(int nrhs) const;
 
@@ -85,7 +93,7 @@ struct Plan : public mxb_plan {
     int setup_split_bf16(const mxb_cds_desc &d);
     void clear_split_graphs();
     int run_split_bf16(const std::vector<Launch> &L, const double *dW, double *dY, int nrhs, int accumulate,
-                       cudaStream_t stream);
+                       cudaStream_t stream, const CallerOrder *order = nullptr);
     void free_split_bf16();
 };
 

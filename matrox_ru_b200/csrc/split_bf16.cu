@@ -120,6 +120,12 @@ struct PlanArgs {
     const int32_t *wofs;
     const int32_t *yofs;
     float *skel;         // FP32 far results awaiting the down launch
+    // caller point order (null: leaf-blocked W / Y at wofs / yofs): tree position t of leaf
+    // i (t from tofs[i]) is row perm[t]; element (row, j) of W at row * w_rs + j * w_cs
+    const int32_t *w_perm;
+    const int32_t *y_perm;
+    const int32_t *tofs;
+    int64_t w_rs, w_cs, y_rs, y_cs;
     int32_t NT;          // 128-column tiles per node in the B buffers (even)
     int32_t nrhs;
     int32_t beta_arg;
@@ -183,7 +189,10 @@ __global__ void __launch_bounds__(256) tile_pool_kernel(const PoolJob *__restric
 }
 
 // W (FP64, leaf-blocked) -> B-operand tiles with 3 parts, for every plan of the launch.
-// B(n, k) = W[k + n ld]; rows n >= nrhs and k >= K are zero.
+// B(n, k) = W[k + n ld]; rows n >= nrhs and k >= K are zero.  ORD: the evaluation reads W in
+// the caller's point order (PlanArgs::w_perm), a separate instantiation so the leaf-blocked
+// one keeps its small footprint.
+template <bool ORD>
 __global__ void __launch_bounds__(256) split_w_kernel(const SplitJob *__restrict__ jobs,
                                                       const PlanArgs *__restrict__ plans)
 {
@@ -192,8 +201,40 @@ __global__ void __launch_bounds__(256) split_w_kernel(const SplitJob *__restrict
     const int kt = blockIdx.y, nt = blockIdx.z;
     if (kt >= j.KT || nt >= pa->NT) return;
     const int nrhs = pa->nrhs;
-    const double *src = pa->W + pa->wofs[j.src_row];
     uint8_t *tile0 = pa->buf[BUF_W] + ((size_t)j.dst_kt * pa->NT + (size_t)nt * j.KT + kt) * 3 * (size_t)TILE_BYTES;
+    if (ORD && pa->w_perm) {
+        // caller point order: gather rows perm[t] of W through shared memory, 64 columns at a
+        // time.  The gather has lanes on consecutive columns (a row-major W is read in 256-byte
+        // runs), the split reads the staged values back in the tile order of the path below.
+        __shared__ double stage[64][65];  // [K index][column]
+        const int32_t *rows = pa->w_perm + pa->tofs[j.src_row];
+        const int64_t rs = pa->w_rs, cs = pa->w_cs;
+        // this thread's 16 K indices: kk = threadIdx.x / 64 + 4 i; its column: threadIdx.x % 64
+        int64_t rofs[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            const int k = kt * 64 + (threadIdx.x >> 6) + 4 * i;
+            rofs[i] = k < j.K ? (int64_t)rows[k] * rs : -1;
+        }
+        for (int half = 0; half < 2; ++half) {
+            const int n = nt * 128 + half * 64 + (threadIdx.x & 63);
+            const double *wc = pa->W + (int64_t)n * cs;
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+                stage[(threadIdx.x >> 6) + 4 * i][threadIdx.x & 63] = (n < nrhs && rofs[i] >= 0) ? wc[rofs[i]] : 0.0;
+            __syncthreads();
+            for (int q = threadIdx.x; q < 64 * 8; q += 256) {
+                const int c = q & 7, rr = q >> 3;
+                __nv_bfloat16 h[8], m[8], l[8];
+#pragma unroll
+                for (int e = 0; e < 8; ++e) tc::split3(stage[c * 8 + e][rr], h[e], m[e], l[e]);
+                store_parts(tile0, 3, half * 64 + rr, c, h, m, l);
+            }
+            __syncthreads();
+        }
+        return;
+    }
+    const double *src = pa->W + pa->wofs[j.src_row];
     for (int i = 0; i < 4; ++i) {
         const int idx = threadIdx.x + i * 256;
         const int c = idx % 8, r = idx / 8;
@@ -282,7 +323,7 @@ struct TcCfg {
 // landed" to the even CTA's pfull barrier, its epilogue warps arrive on the even CTA's acce
 // barrier, and the even CTA's commits arrive on both CTAs' barriers.  A failed wait in either
 // CTA sets both CTAs' abort words.
-template <int P, int BN, int STAGES_, bool PAIR>
+template <int P, int BN, int STAGES_, bool PAIR, bool ORD>
 __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_gemm_kernel(LaunchArgs la)
 {
     using C = TcCfg<P, BN, STAGES_, PAIR>;
@@ -590,9 +631,21 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                 const int beta = t.beta == 2 ? pa->beta_arg : t.beta;
                 const int nrhs = pa->nrhs;
                 const char *f32 = nullptr, *f64 = nullptr;
-                if (t.out_kind == OUT_Y && beta) f64 = reinterpret_cast<const char *>(pa->Y + pa->yofs[t.c_row] + r0);
-                else if (t.out_kind == OUT_TILES && beta)
+                if (ORD && t.out_kind == OUT_Y && beta && pa->y_perm) {
+                    // caller point order: each lane asks for its own row's columns when they
+                    // are contiguous (one 128-byte line per 16 columns)
+                    const int rl = r0 + lane;
+                    if (rl < t.M && pa->y_cs == 1) {
+                        const char *q = reinterpret_cast<const char *>(
+                            pa->Y + (int64_t)pa->y_perm[pa->tofs[t.c_row] + rl] * pa->y_rs + c0);
+                        const int ncol = min(C::COLS, nrhs - c0);
+                        for (int j = 0; j < ncol; j += 16) asm volatile("prefetch.global.L2 [%0];\n" ::"l"(q + j * 8));
+                    }
+                } else if (t.out_kind == OUT_Y && beta) {
+                    f64 = reinterpret_cast<const char *>(pa->Y + pa->yofs[t.c_row] + r0);
+                } else if (t.out_kind == OUT_TILES && beta) {
                     f32 = reinterpret_cast<const char *>(pa->skel + t.c_row * (int64_t)nrhs + r0);
+                }
                 if (r0 < t.M && (f32 || f64)) {
                     for (int j = lane; j < C::COLS; j += 32) {
                         const int cc = c0 + j;
@@ -648,7 +701,57 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
             const int col0 = un.col * BN + half * C::COLS;
             // accumulating outputs: all old values of a 16-column chunk are loaded before any
             // store, so the loads overlap instead of waiting on each other
-            if (t.out_kind == OUT_Y) {
+            if (ORD && t.out_kind == OUT_Y && pa->y_perm) {
+                // caller point order: row t of the leaf goes to row perm[t] of Y.  An 8 x 8
+                // transpose inside each group of 8 lanes gives every lane one column of 8
+                // consecutive tree rows, so each access covers 8 columns (64 bytes) of a row, 4
+                // rows per warp instruction, instead of 32 rows.  All lanes take part in the
+                // shuffles; rows past M are masked at the accesses.
+                const int rg = t.m0 + (int)rank * 128 + quarter * 32 + (lane & ~7);  // group's first row
+                const int rows_ok = t.M - rg;  // rows rg + j with j < rows_ok exist
+                // lane 8g + i holds the element offset of caller row perm[rg + i]; the others
+                // shuffle it
+                const int64_t roff =
+                    (lane & 7) < rows_ok ? (int64_t)pa->y_perm[pa->tofs[t.c_row] + rg + (lane & 7)] * pa->y_rs : 0;
+                const int64_t ycs = pa->y_cs;
+                double *ycol = pa->Y + (int64_t)(col0 + (lane & 7)) * ycs;  // advances 8 columns a group
+                // per batch: GB column groups x JB rows of old values in flight (fewer where 128
+                // accumulators already fill the registers)
+                constexpr int GB = C::COLS >= 128 ? 1 : 2;
+                constexpr int JB = C::COLS >= 128 ? 4 : 8;
+#pragma unroll
+                for (int g8 = 0; g8 < C::COLS / 8; g8 += GB) {
+                    float x[GB][8];
+#pragma unroll
+                    for (int gb = 0; gb < GB; ++gb) {
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) x[gb][j] = acc[8 * (g8 + gb) + j];
+                        transpose8(x[gb], lane);  // x[gb][j]: row rg + j, column col0 + 8 (g8 + gb) + (lane & 7)
+                    }
+#pragma unroll
+                    for (int j0 = 0; j0 < 8; j0 += JB) {
+                        int64_t ro[JB];
+                        double old[GB][JB];
+#pragma unroll
+                        for (int j = 0; j < JB; ++j) ro[j] = __shfl_sync(0xffffffffu, roff, (lane & ~7) | (j0 + j));
+#pragma unroll
+                        for (int gb = 0; gb < GB; ++gb) {
+                            const bool col_ok = col0 + 8 * (g8 + gb) + (lane & 7) < nrhs;
+#pragma unroll
+                            for (int j = 0; j < JB; ++j)
+                                old[gb][j] = (beta && col_ok && j0 + j < rows_ok) ? ycol[ro[j] + 8 * gb * ycs] : 0.0;
+                        }
+#pragma unroll
+                        for (int gb = 0; gb < GB; ++gb) {
+                            const bool col_ok = col0 + 8 * (g8 + gb) + (lane & 7) < nrhs;
+#pragma unroll
+                            for (int j = 0; j < JB; ++j)
+                                if (col_ok && j0 + j < rows_ok) ycol[ro[j] + 8 * gb * ycs] = old[gb][j] + (double)x[gb][j0 + j];
+                        }
+                    }
+                    ycol += 8 * GB * ycs;
+                }
+            } else if (t.out_kind == OUT_Y) {
                 if (r < t.M) {
                     double *Yb = pa->Y + pa->yofs[t.c_row] + r;
 #pragma unroll
@@ -750,7 +853,7 @@ int sm_count()
     return g_sm_count[dev];
 }
 
-template <int P, int BN, int S, bool PAIR>
+template <int P, int BN, int S, bool PAIR, bool ORD>
 cudaError_t configure_tc()
 {
     static bool done[128];
@@ -759,22 +862,22 @@ cudaError_t configure_tc()
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 128) return cudaErrorInvalidDevice;
     if (done[dev]) return cudaSuccess;
-    e = cudaFuncSetAttribute(tc_gemm_kernel<P, BN, S, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(tc_gemm_kernel<P, BN, S, PAIR, ORD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              TcCfg<P, BN, S, PAIR>::SMEM);
     if (e == cudaSuccess) done[dev] = true;
     return e;
 }
 
-template <int P, int BN, int S, bool PAIR>
+template <int P, int BN, int S, bool PAIR, bool ORD>
 cudaError_t launch_tc_cfg(const LaunchArgs &a, cudaStream_t s)
 {
     using C = TcCfg<P, BN, S, PAIR>;
     if (a.nunits <= 0) return cudaSuccess;
-    cudaError_t e = configure_tc<P, BN, S, PAIR>();
+    cudaError_t e = configure_tc<P, BN, S, PAIR, ORD>();
     if (e != cudaSuccess) return e;
     if constexpr (!PAIR) {
         const int grid = std::min(a.nunits, sm_count());
-        tc_gemm_kernel<P, BN, S, false><<<grid, C::THREADS, C::SMEM, s>>>(a);
+        tc_gemm_kernel<P, BN, S, false, ORD><<<grid, C::THREADS, C::SMEM, s>>>(a);
         return cudaGetLastError();
     } else {
         const int pairs = std::min(a.nunits, std::max(1, sm_count() / 2));
@@ -790,39 +893,55 @@ cudaError_t launch_tc_cfg(const LaunchArgs &a, cudaStream_t s)
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        return cudaLaunchKernelEx(&cfg, tc_gemm_kernel<P, BN, S, true>, a);
+        return cudaLaunchKernelEx(&cfg, tc_gemm_kernel<P, BN, S, true, ORD>, a);
     }
 }
 
 // Column-tile widths per product count; pipeline depth fills ~192-216 KiB of shared memory.
 // A pair stages half of B per CTA, which buys a deeper pipeline at the same width.
-cudaError_t launch_tc(int P, int BN, bool pair, const LaunchArgs &a, cudaStream_t s)
+template <bool ORD>
+cudaError_t launch_tc_ord(int P, int BN, bool pair, const LaunchArgs &a, cudaStream_t s)
 {
     if (pair) {
-        if (P == 2) return BN == 256 ? launch_tc_cfg<2, 256, 3, true>(a, s) : launch_tc_cfg<2, 128, 4, true>(a, s);
-        return BN == 256 ? launch_tc_cfg<3, 256, 2, true>(a, s) : launch_tc_cfg<3, 128, 3, true>(a, s);
+        if (P == 2)
+            return BN == 256 ? launch_tc_cfg<2, 256, 3, true, ORD>(a, s) : launch_tc_cfg<2, 128, 4, true, ORD>(a, s);
+        return BN == 256 ? launch_tc_cfg<3, 256, 2, true, ORD>(a, s) : launch_tc_cfg<3, 128, 3, true, ORD>(a, s);
     }
     if (P == 2) {
-        if (BN == 256) return launch_tc_cfg<2, 256, 2, false>(a, s);
-        if (BN == 128) return launch_tc_cfg<2, 128, 3, false>(a, s);
-        return launch_tc_cfg<2, 64, 4, false>(a, s);
+        if (BN == 256) return launch_tc_cfg<2, 256, 2, false, ORD>(a, s);
+        if (BN == 128) return launch_tc_cfg<2, 128, 3, false, ORD>(a, s);
+        return launch_tc_cfg<2, 64, 4, false, ORD>(a, s);
     }
-    if (BN == 128) return launch_tc_cfg<3, 128, 2, false>(a, s);
-    return launch_tc_cfg<3, 64, 3, false>(a, s);
+    if (BN == 128) return launch_tc_cfg<3, 128, 2, false, ORD>(a, s);
+    return launch_tc_cfg<3, 64, 3, false, ORD>(a, s);
+}
+
+// ord: the launch writes Y in the caller's point order (the instantiation with the scatter
+// epilogue); every other launch runs the leaf-blocked one.
+cudaError_t launch_tc(int P, int BN, bool pair, bool ord, const LaunchArgs &a, cudaStream_t s)
+{
+    return ord ? launch_tc_ord<true>(P, BN, pair, a, s) : launch_tc_ord<false>(P, BN, pair, a, s);
+}
+
+template <bool ORD>
+cudaError_t configure_all_tc_ord()
+{
+    cudaError_t e = configure_tc<2, 256, 2, false, ORD>();
+    if (e == cudaSuccess) e = configure_tc<2, 128, 3, false, ORD>();
+    if (e == cudaSuccess) e = configure_tc<2, 64, 4, false, ORD>();
+    if (e == cudaSuccess) e = configure_tc<3, 128, 2, false, ORD>();
+    if (e == cudaSuccess) e = configure_tc<3, 64, 3, false, ORD>();
+    if (e == cudaSuccess) e = configure_tc<2, 256, 3, true, ORD>();
+    if (e == cudaSuccess) e = configure_tc<2, 128, 4, true, ORD>();
+    if (e == cudaSuccess) e = configure_tc<3, 256, 2, true, ORD>();
+    if (e == cudaSuccess) e = configure_tc<3, 128, 3, true, ORD>();
+    return e;
 }
 
 cudaError_t configure_all_tc()
 {
-    cudaError_t e = configure_tc<2, 256, 2, false>();
-    if (e == cudaSuccess) e = configure_tc<2, 128, 3, false>();
-    if (e == cudaSuccess) e = configure_tc<2, 64, 4, false>();
-    if (e == cudaSuccess) e = configure_tc<3, 128, 2, false>();
-    if (e == cudaSuccess) e = configure_tc<3, 64, 3, false>();
-    if (e == cudaSuccess) e = configure_tc<2, 256, 3, true>();
-    if (e == cudaSuccess) e = configure_tc<2, 128, 4, true>();
-    if (e == cudaSuccess) e = configure_tc<3, 256, 2, true>();
-    if (e == cudaSuccess) e = configure_tc<3, 128, 3, true>();
-    return e;
+    cudaError_t e = configure_all_tc_ord<false>();
+    return e == cudaSuccess ? configure_all_tc_ord<true>() : e;
 }
 
 int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
@@ -893,6 +1012,7 @@ struct Batch : public mxb_batch {
         int first, count;  // range in the merged tasks or jobs
         int max_kt;
         int max_m;         // tallest output block (pairs only pay off above 128 rows)
+        bool writes_y;     // some task writes Y (the launch scatters rows in caller order)
     };
     std::vector<MOp> ops;
     std::vector<TcTask> tasks;
@@ -910,6 +1030,7 @@ struct Batch : public mxb_batch {
         int accumulate = 0;
         int debug_flags = 0;
         std::vector<int> bn;           // column-tile width per op (0 for the W split)
+        std::vector<CallerOrder> order;  // per plan, when W / Y are in the caller's point order
         PlanArgs *dPlans = nullptr;
         TcUnit *dUnits = nullptr;
         std::vector<int> unit_first, unit_count;
@@ -942,13 +1063,13 @@ struct Batch : public mxb_batch {
     }
     int build(const std::vector<Plan *> &ps);
     int evaluate(const double *const *W, double *const *Y, const int *nrhs, int accumulate, cudaStream_t stream,
-                 int debug_flags, long long wait_cycles);
+                 int debug_flags, long long wait_cycles, const CallerOrder *order = nullptr);
     int enqueue(Entry &e, cudaStream_t stream, int debug_flags, long long wait_cycles, const std::vector<int> &bn,
                 int only_op = -1);
     int units_for(Entry &e, const std::vector<int> &bn, cudaStream_t stream);
     int tune(Entry &e, std::vector<PlanArgs> pa, std::vector<int> &bn, cudaStream_t stream, long long wait_cycles);
     Entry *find(const double *const *W, double *const *Y, const std::vector<int> &nr, int accumulate,
-                int debug_flags);
+                int debug_flags, const CallerOrder *order = nullptr);
     int profile(const double *const *W, double *const *Y, const int *nrhs, cudaStream_t stream, mxb_op_profile *out,
                 int cap, int *nops);
 };
@@ -1001,6 +1122,7 @@ int Batch::build(const std::vector<Plan *> &ps)
                     t.item0 = item0;
                     t.plan = po.first;
                     m.max_m = std::max(m.max_m, t.M);
+                    m.writes_y |= t.out_kind == OUT_Y;
                     tasks.push_back(t);
                 }
             }
@@ -1088,7 +1210,10 @@ int Batch::enqueue(Entry &e, cudaStream_t stream, int debug_flags, long long wai
         cudaError_t err = cudaSuccess;
         if (m.phase == PH_SPLITW) {
             if (run) {
-                split_w_kernel<<<dim3(m.count, m.max_kt, maxnt), 256, 0, stream>>>(dJobs + m.first, e.dPlans);
+                if (e.order.empty())
+                    split_w_kernel<false><<<dim3(m.count, m.max_kt, maxnt), 256, 0, stream>>>(dJobs + m.first, e.dPlans);
+                else
+                    split_w_kernel<true><<<dim3(m.count, m.max_kt, maxnt), 256, 0, stream>>>(dJobs + m.first, e.dPlans);
                 err = cudaGetLastError();
             }
         } else {
@@ -1104,7 +1229,7 @@ int Batch::enqueue(Entry &e, cudaStream_t stream, int debug_flags, long long wai
                 a.wait_cycles = wait_cycles > 0 ? wait_cycles : tc::WAIT_CYCLES;
                 a.stall_test = (debug_flags & MXB_DEBUG_STALL_ONE_WAIT) && first_tc;
                 a.kchain = kchain_for(m.P);
-                err = launch_tc(m.P, tile_width(bn[k]), tile_pair(bn[k]), a, stream);
+                err = launch_tc(m.P, tile_width(bn[k]), tile_pair(bn[k]), m.writes_y && !e.order.empty(), a, stream);
             }
             first_tc = false;
         }
@@ -1206,6 +1331,7 @@ int Batch::tune(Entry &e, std::vector<PlanArgs> pa, std::vector<int> &bn, cudaSt
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     Entry te;
     te.nrhs = e.nrhs;
+    te.order = e.order;  // the same kernel instantiations as the evaluation (Y goes to scratch)
     int rc = MXB_OK;
     for (int i = 0; i < np && !rc; ++i) {
         Plan &p = *plans[i];
@@ -1216,6 +1342,7 @@ int Batch::tune(Entry &e, std::vector<PlanArgs> pa, std::vector<int> &bn, cudaSt
             rc = batch_fail("autotune scratch allocation failed", MXB_ERR_NOMEM);
         else
             pa[i].Y = scratch[i];
+        pa[i].y_perm = nullptr;  // the scratch is leaf-blocked (packed offsets)
     }
     if (!rc && cudaMalloc(&dTune, np * sizeof(PlanArgs)) != cudaSuccess)
         rc = batch_fail("autotune table allocation failed", MXB_ERR_NOMEM);
@@ -1280,7 +1407,7 @@ int Batch::tune(Entry &e, std::vector<PlanArgs> pa, std::vector<int> &bn, cudaSt
 }
 
 int Batch::evaluate(const double *const *W, double *const *Y, const int *nrhs, int accumulate, cudaStream_t stream,
-                    int debug_flags, long long wait_cycles)
+                    int debug_flags, long long wait_cycles, const CallerOrder *order)
 {
     const int np = (int)plans.size();
     int cur = -1;
@@ -1297,7 +1424,7 @@ int Batch::evaluate(const double *const *W, double *const *Y, const int *nrhs, i
     }
     if (realloc) clear();
     MXB_CUDA_OR(configure_all_tc());
-    Entry *hit = find(W, Y, nr, accumulate, debug_flags);
+    Entry *hit = find(W, Y, nr, accumulate, debug_flags, order);
     if (!hit) {
         if (entries.size() >= 8) {
             release(entries.front());
@@ -1309,6 +1436,7 @@ int Batch::evaluate(const double *const *W, double *const *Y, const int *nrhs, i
         e.nrhs = nr;
         e.accumulate = accumulate;
         e.debug_flags = debug_flags;
+        if (order) e.order.assign(order, order + np);
         std::vector<PlanArgs> pa(np);
         for (int i = 0; i < np; ++i) {
             Plan &p = *plans[i];
@@ -1325,6 +1453,14 @@ int Batch::evaluate(const double *const *W, double *const *Y, const int *nrhs, i
             pa[i].NT = S.nt_cap;
             pa[i].nrhs = nr[i];
             pa[i].beta_arg = accumulate ? 1 : 0;
+            if (order) {
+                pa[i].w_perm = pa[i].y_perm = order[i].perm;
+                pa[i].tofs = order[i].tofs;
+                pa[i].w_rs = order[i].w_rs;
+                pa[i].w_cs = order[i].w_cs;
+                pa[i].y_rs = order[i].y_rs;
+                pa[i].y_cs = order[i].y_cs;
+            }
         }
         cudaError_t err = cudaMalloc(&e.dPlans, np * sizeof(PlanArgs));
         // on the evaluation stream, ahead of the graph launch that reads it
@@ -1389,11 +1525,17 @@ int Batch::evaluate(const double *const *W, double *const *Y, const int *nrhs, i
 }
 
 Batch::Entry *Batch::find(const double *const *W, double *const *Y, const std::vector<int> &nr, int accumulate,
-                          int debug_flags)
+                          int debug_flags, const CallerOrder *order)
 {
     Entry *hit = nullptr;
     for (Entry &e : entries) {
-        bool same = e.accumulate == accumulate && e.nrhs == nr && e.debug_flags == debug_flags;
+        bool same = e.accumulate == accumulate && e.nrhs == nr && e.debug_flags == debug_flags &&
+                    e.order.empty() == !order;
+        for (size_t i = 0; same && order && i < plans.size(); ++i) {
+            const CallerOrder &a = e.order[i], &b = order[i];
+            same = a.perm == b.perm && a.tofs == b.tofs && a.w_rs == b.w_rs && a.w_cs == b.w_cs && a.y_rs == b.y_rs &&
+                   a.y_cs == b.y_cs;
+        }
         for (size_t i = 0; same && i < plans.size(); ++i) same = e.W[i] == W[i] && e.Y[i] == Y[i];
         if (same) hit = &e;
     }
@@ -1708,13 +1850,13 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
 }
 
 int Plan::run_split_bf16(const std::vector<Launch> &L, const double *dW, double *dY, int nrhs, int accumulate,
-                         cudaStream_t stream)
+                         cudaStream_t stream, const CallerOrder *order)
 {
     if (&L == &launches_adj) {
         set_error("the adjoint runs in FP64 mode only (create an FP64 plan for mxb_plan_adjoint)");
         return MXB_ERR_UNSUPPORTED;
     }
-    return bf16->self->evaluate(&dW, &dY, &nrhs, accumulate, stream, debug_flags, debug_wait_cycles);
+    return bf16->self->evaluate(&dW, &dY, &nrhs, accumulate, stream, debug_flags, debug_wait_cycles, order);
 }
 
 void Plan::clear_split_graphs()

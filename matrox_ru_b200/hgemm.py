@@ -320,6 +320,40 @@ class Plan:
                                            recs, 4096, ctypes.byref(n)), "mxb_plan_profile")
         return _profile_records(recs, n.value)
 
+    def set_permutation(self, perm) -> None:
+        """Register the caller's point order: perm[t] is the row of W / Y that holds tree
+        position t (``CDS.perm``, the reference's ``lids``)."""
+        perm = np.ascontiguousarray(perm, dtype=np.int32)
+        if perm.shape != (self.n,):
+            raise ValueError("perm must have one entry per point")
+        check(_lib.load().mxb_plan_set_permutation(self._h, perm.ctypes.data), "mxb_plan_set_permutation")
+
+    def _ordered(self, fn, name, W, out, accumulate, stream):
+        torch = _torch()
+        if not (W.is_cuda and W.dtype == torch.float64 and W.dim() == 2 and W.shape[0] == self.n):
+            raise TypeError("operands must be (N, r) float64 CUDA tensors")
+        r = W.shape[1]
+        if out is None:
+            out = torch.empty((self.n, r), dtype=torch.float64, device=W.device)
+            accumulate = False
+        if not (out.is_cuda and out.dtype == torch.float64 and tuple(out.shape) == (self.n, r)):
+            raise TypeError("out must be an (N, r) float64 CUDA tensor")
+        check(fn(self._h, W.data_ptr(), W.stride(0), W.stride(1), out.data_ptr(), out.stride(0), out.stride(1), r,
+                 int(accumulate), _stream_ptr(stream)), name)
+        return out
+
+    def evaluate_ordered(self, W, out=None, accumulate: bool = False, stream=None):
+        """out (+)= K~ W with W, out as (N, r) float64 CUDA tensors in the caller's point
+        order (any non-overlapping strides).  Split-BF16 plans gather and scatter the rows
+        inside their own launches; ``set_permutation`` must have been called."""
+        return self._ordered(_lib.load().mxb_plan_evaluate_ordered, "mxb_plan_evaluate_ordered", W, out,
+                             accumulate, stream)
+
+    def adjoint_ordered(self, G, out=None, accumulate: bool = False, stream=None):
+        """out (+)= K~^T G in the caller's point order (FP64 plans)."""
+        return self._ordered(_lib.load().mxb_plan_adjoint_ordered, "mxb_plan_adjoint_ordered", G, out,
+                             accumulate, stream)
+
     def adjoint(self, TG, nrhs: int, out=None, accumulate: bool = False, stream=None):
         """out (+)= K~^T TG (packed leaf-blocked float64 CUDA tensors)."""
         torch = _torch()
@@ -404,9 +438,10 @@ class Batch:
 class Evaluator:
     """Y = K~ W with W, Y as (N, r) float64 CUDA tensors in the caller's point order."""
 
-    def __init__(self, cds, precision: str = "fp64"):
+    def __init__(self, cds, precision: str = "fp64", plan: Optional[Plan] = None):
         torch = _torch()
-        self.plan = Plan(cds, precision)
+        self.plan = plan if plan is not None else Plan(cds, precision)
+        self.plan.set_permutation(cds.perm)
         self.cds = cds
         dev = torch.device("cuda", self.plan.device)
         self.perm = torch.as_tensor(cds.perm.astype(np.int32), device=dev)
@@ -448,14 +483,10 @@ class Evaluator:
         torch = _torch()
         if W.dtype != torch.float64 or not W.is_cuda or W.dim() != 2 or W.shape[0] != self.cds.n:
             raise TypeError("W must be an (N, r) float64 CUDA tensor")
-        r = W.shape[1]
-        TY = self.plan.evaluate(self.to_tree(W, stream), r, stream=stream)
-        return self.from_tree(TY, r, stream=stream)
+        return self.plan.evaluate_ordered(W, stream=stream)
 
     def adjoint(self, G, stream=None):
-        r = G.shape[1]
-        TGW = self.plan.adjoint(self.to_tree(G, stream), r, stream=stream)
-        return self.from_tree(TGW, r, stream=stream)
+        return self.plan.adjoint_ordered(G, stream=stream)
 
 
 def kernel_matvec(evaluator: Evaluator, W):
