@@ -31,10 +31,19 @@ __global__ void permute_kernel(const int32_t *__restrict__ perm, const int32_t *
                                int64_t cs, int nrhs, int dir, int accumulate)
 {
     __shared__ double tile[T][T + 1];  // [position][column]
+    __shared__ int64_t qbase[T];       // leaf-blocked offset of each position's column 0
+    __shared__ int32_t qld[T];         // its leaf's row count (the block's leading dimension)
     const int64_t t0 = (int64_t)blockIdx.x * T;
     const int j0 = blockIdx.y * T;
     const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
     const bool caller_j_fast = cs < rs;
+    if (ty == 0 && t0 + tx < n) {  // one leaf lookup per position, not per element
+        const int64_t t = t0 + tx;
+        const int leaf = leaf_of(leafofs, nleaf, t);
+        qbase[tx] = (int64_t)blockofs[leaf] + (t - leafofs[leaf]);
+        qld[tx] = leafofs[leaf + 1] - leafofs[leaf];
+    }
+    __syncthreads();
     for (int phase = 0; phase < 2; ++phase) {
         const bool caller_side = (phase == 0) == (dir == 0);
         const bool j_fast = caller_side && caller_j_fast;
@@ -49,9 +58,7 @@ __global__ void permute_kernel(const int32_t *__restrict__ perm, const int32_t *
                 if (phase == 0) tile[a][b] = src[p];
                 else dst[p] = accumulate ? dst[p] + tile[a][b] : tile[a][b];
             } else {
-                const int leaf = leaf_of(leafofs, nleaf, t);
-                const int64_t m = leafofs[leaf + 1] - leafofs[leaf];
-                const int64_t q = (int64_t)blockofs[leaf] + (int64_t)j * m + (t - leafofs[leaf]);
+                const int64_t q = qbase[a] + (int64_t)j * qld[a];
                 if (phase == 0) tile[a][b] = src[q];
                 else dst[q] = tile[a][b];
             }

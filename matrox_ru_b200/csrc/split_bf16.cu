@@ -203,32 +203,33 @@ __global__ void __launch_bounds__(256) split_w_kernel(const SplitJob *__restrict
     const int nrhs = pa->nrhs;
     uint8_t *tile0 = pa->buf[BUF_W] + ((size_t)j.dst_kt * pa->NT + (size_t)nt * j.KT + kt) * 3 * (size_t)TILE_BYTES;
     if (ORD && pa->w_perm) {
-        // caller point order: gather rows perm[t] of W through shared memory, 64 columns at a
-        // time.  The gather has lanes on consecutive columns (a row-major W is read in 256-byte
-        // runs), the split reads the staged values back in the tile order of the path below.
-        __shared__ double stage[64][65];  // [K index][column]
+        // caller point order: gather rows perm[t] of W through shared memory, 32 K indices
+        // (rows of W) at a time across all 128 columns of the tile.  Lanes run along a row, so
+        // a row-major W is read in 1 KiB runs; the split then reads the staged values back in
+        // the tile order of the path below (chunks 4 h .. 4 h + 3 of every tile row).
+        __shared__ double stage[32][129];  // [K index][column]
         const int32_t *rows = pa->w_perm + pa->tofs[j.src_row];
         const int64_t rs = pa->w_rs, cs = pa->w_cs;
-        // this thread's 16 K indices: kk = threadIdx.x / 64 + 4 i; its column: threadIdx.x % 64
-        int64_t rofs[16];
+        const int n = nt * 128 + (threadIdx.x & 127);
+        const double *wc = pa->W + (int64_t)n * cs;
+        for (int h = 0; h < 2; ++h) {
+            // this thread's 16 K indices: kk = threadIdx.x / 128 + 2 i; its column: threadIdx.x % 128
+            int64_t rofs[16];
 #pragma unroll
-        for (int i = 0; i < 16; ++i) {
-            const int k = kt * 64 + (threadIdx.x >> 6) + 4 * i;
-            rofs[i] = k < j.K ? (int64_t)rows[k] * rs : -1;
-        }
-        for (int half = 0; half < 2; ++half) {
-            const int n = nt * 128 + half * 64 + (threadIdx.x & 63);
-            const double *wc = pa->W + (int64_t)n * cs;
+            for (int i = 0; i < 16; ++i) {
+                const int k = kt * 64 + h * 32 + (threadIdx.x >> 7) + 2 * i;
+                rofs[i] = k < j.K ? (int64_t)rows[k] * rs : -1;
+            }
 #pragma unroll
             for (int i = 0; i < 16; ++i)
-                stage[(threadIdx.x >> 6) + 4 * i][threadIdx.x & 63] = (n < nrhs && rofs[i] >= 0) ? wc[rofs[i]] : 0.0;
+                stage[(threadIdx.x >> 7) + 2 * i][threadIdx.x & 127] = (n < nrhs && rofs[i] >= 0) ? wc[rofs[i]] : 0.0;
             __syncthreads();
-            for (int q = threadIdx.x; q < 64 * 8; q += 256) {
-                const int c = q & 7, rr = q >> 3;
-                __nv_bfloat16 h[8], m[8], l[8];
+            for (int q = threadIdx.x; q < 128 * 4; q += 256) {
+                const int c = q & 3, rr = q >> 2;
+                __nv_bfloat16 hi[8], mi[8], lo[8];
 #pragma unroll
-                for (int e = 0; e < 8; ++e) tc::split3(stage[c * 8 + e][rr], h[e], m[e], l[e]);
-                store_parts(tile0, 3, half * 64 + rr, c, h, m, l);
+                for (int e = 0; e < 8; ++e) tc::split3(stage[c * 8 + e][rr], hi[e], mi[e], lo[e]);
+                store_parts(tile0, 3, rr, h * 4 + c, hi, mi, lo);
             }
             __syncthreads();
         }
