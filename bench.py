@@ -431,6 +431,22 @@ def main():
                       "max_rel_diff_vs_host_assembly": diff}
         del dD, dB
         torch.cuda.empty_cache()
+    # the same CDS built with the ID compression on the GPU (mxb_batched_id, one launch per tree
+    # level) instead of one host ID per node; the tree, sampling and block assembly stay the same
+    gpu_id = None
+    if rank == 0 and world == 1:
+        from matrox_ru_b200 import structure as S
+        t0 = time.time()
+        cg = S.build_cds(X, S_kernel_spec(cfg), leaf_size=cfg["leaf"], budget=cfg["budget"], tol=cfg["tol"],
+                         max_rank=cfg["max_rank"], seed=cfg["seed"], id_on_gpu=True)
+        tg = time.time() - t0
+        nodes = range(1, cds.numnodes)
+        gpu_id = {"cds_build_s": round(tg, 1), "host_id_cds_build_s": round(t_build, 1),
+                  "nodes_same_rank": float(np.mean([cds.slen[v] == cg.slen[v] for v in nodes])),
+                  "nodes_same_skeleton": float(np.mean([np.array_equal(np.sort(cds.skels[v]), np.sort(cg.skels[v]))
+                                                        for v in nodes]))}
+        del cg
+        torch.cuda.empty_cache()
     # tensor-core flops each split mode executes: 3 or 6 bf16 products per algorithmic product
     exec_flops = {"fp64": flops,
                   "split_bf16": 3 * (fb["near"] + fb["far"]) + 6 * fb["tree"],
@@ -644,7 +660,7 @@ def main():
         "gflops": round(flops / (ms * 1e-3) / 1e9, 1),
         "aggregate_gflops": round(world * flops / (ms * 1e-3) / 1e9, 1),
         "modes": results, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-        "clocks": clocks, "cds_build_s": round(t_build, 1), "gpu_cds_blocks": gpu_blocks,
+        "clocks": clocks, "cds_build_s": round(t_build, 1), "gpu_cds_blocks": gpu_blocks, "gpu_id_cds_build": gpu_id,
     }
     if rank == 0:
         print(json.dumps(line))

@@ -332,6 +332,22 @@ MXB_API int32_t mxb_kernel_blocks(const double *dX, int64_t n, int32_t d, int32_
                                   const int32_t *blk_row, const int32_t *blk_col, const uint64_t *blk_ofs,
                                   int32_t nblk, double *dOut, uint64_t out_len, void *stream);
 
+/* ---- ID compression on the GPU ------------------------------------------------------------ */
+
+/* Replaces the per-node host ID of the CDS build, matroxTest-V1/compression.h:446-523
+ * (`decomposition`: LAPACKE_dgeqp3, the rank rule, cblas_dtrsm).  count sample matrices A_b
+ * (nrows[b] x ncols[b], column-major, packed back to back in dA, which is overwritten) are
+ * factored in one launch, one CTA per matrix: Householder QR with column pivoting, rank
+ * s_b = the first s >= 1 with |R[s,s] / R[0,0]| < tol (at most max_rank and min(nrows, ncols)),
+ * and P_b (s_b x ncols[b]) with R11 P_b[:, piv] = R[0:s_b, :].  Outputs (device arrays):
+ * dRank[b] = s_b; dPiv holds ncols[b] pivots per matrix, packed (the first s_b are the
+ * skeleton columns); dP holds min(max_rank, ncols[b]) x ncols[b] doubles per matrix, packed,
+ * of which the first s_b x ncols[b] are P_b (column-major, leading dimension s_b).
+ * ncols <= 8192.  Asynchronous on `stream`. */
+MXB_API int32_t mxb_batched_id(double *dA, const int32_t *nrows, const int32_t *ncols, int32_t count,
+                               double tol, int32_t max_rank, int32_t *dRank, int32_t *dPiv, double *dP,
+                               void *stream);
+
 /* ---- evaluation without device allocation ------------------------------------------------ */
 
 /* No counterpart in the reference (its evaluator runs on the host).  For callers that may

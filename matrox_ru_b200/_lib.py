@@ -113,6 +113,7 @@ def load(path: str = LIB_PATH):
     lib.mxb_transform.argtypes = [P, P, P, I32, P, I64, I64, I32, P]
     lib.mxb_untransform.argtypes = [P, P, P, I32, P, I64, I64, I32, P]
     lib.mxb_evaluate_noalloc.argtypes = [ctypes.POINTER(CdsDesc), P, P, I32, I32, P]
+    lib.mxb_batched_id.argtypes = [P, P, P, I32, ctypes.c_double, I32, P, P, P, P]
     lib.mxb_kernel_blocks.argtypes = [P, I64, I32, I32, ctypes.c_double, P, P, I32, P, P, P, I32, P, U64, P]
     lib.mxb_hgemm_set_shape.argtypes = [I32, I32, I32]
     lib.mxb_hgemm_hss_set_shape.argtypes = [I32, I32]

@@ -227,6 +227,62 @@ def kernel_blocks(cds, X, kernel, stream=None):
     return out[0], out[1]
 
 
+def kernel_matrices(dX, kernel, row_sets, col_sets, stream=None):
+    """Kernel blocks K(X[rows_b], X[cols_b]) for every pair of index sets, computed on the GPU
+    (``mxb_kernel_blocks``) and packed back to back, each column-major.  dX: (N, d) float64
+    CUDA tensor.  Returns (pool, offsets)."""
+    torch = _torch()
+    n, d = dX.shape
+    sets = [np.asarray(x, dtype=np.int64) for x in row_sets] + [np.asarray(x, dtype=np.int64) for x in col_sets]
+    nb = len(row_sets)
+    set_ofs = np.concatenate([[0], np.cumsum([len(x) for x in sets])]).astype(np.int64)
+    set_idx = np.concatenate(sets).astype(np.int32) if set_ofs[-1] else np.zeros(1, np.int32)
+    sizes = np.array([len(r) * len(c) for r, c in zip(row_sets, col_sets)], np.int64)
+    ofs = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.uint64)
+    total = int(sizes.sum())
+    dst = torch.empty(max(total, 1), dtype=torch.float64, device=dX.device)
+    a = _Args()
+    check(_lib.load().mxb_kernel_blocks(dX.data_ptr(), n, d, _lib.KERNEL_KINDS[kernel.kind], float(kernel.h),
+                                        a(set_ofs, np.int64), a(set_idx), len(sets),
+                                        a(np.arange(nb, dtype=np.int32)), a(np.arange(nb, 2 * nb, dtype=np.int32)),
+                                        a(ofs, np.uint64), nb, dst.data_ptr(), total, _stream_ptr(stream)),
+          "mxb_kernel_blocks")
+    return dst, ofs
+
+
+def batched_id(pool, shapes, tol: float, max_rank: int, stream=None):
+    """Column IDs of the packed column-major matrices in ``pool`` (a float64 CUDA tensor,
+    overwritten), ``shapes`` = [(nrows, ncols), ...], on the GPU (``mxb_batched_id``).  Returns a
+    list of (skeleton column positions, P) as numpy arrays, like
+    :func:`matrox_ru_b200.structure.interpolative_decomposition`."""
+    torch = _torch()
+    if not shapes:
+        return []
+    nr = np.array([r for r, _ in shapes], np.int32)
+    nc = np.array([c for _, c in shapes], np.int32)
+    if not (pool.is_cuda and pool.dtype == torch.float64 and pool.is_contiguous()):
+        raise TypeError("pool must be a contiguous float64 CUDA tensor")
+    if pool.numel() < int((nr.astype(np.int64) * nc).sum()):
+        raise ValueError("pool smaller than the matrices it should hold")
+    pmax = np.minimum(max_rank, nc).astype(np.int64)
+    dRank = torch.empty(len(shapes), dtype=torch.int32, device=pool.device)
+    dPiv = torch.empty(int(nc.sum()), dtype=torch.int32, device=pool.device)
+    dP = torch.empty(max(int((pmax * nc).sum()), 1), dtype=torch.float64, device=pool.device)
+    check(_lib.load().mxb_batched_id(pool.data_ptr(), nr.ctypes.data, nc.ctypes.data, len(shapes), float(tol),
+                                     int(max_rank), dRank.data_ptr(), dPiv.data_ptr(), dP.data_ptr(),
+                                     _stream_ptr(stream)), "mxb_batched_id")
+    ranks = dRank.cpu().numpy()
+    piv = dPiv.cpu().numpy()
+    Pall = dP.cpu().numpy()
+    out, q, p = [], 0, 0
+    for b in range(len(shapes)):
+        s, c = int(ranks[b]), int(nc[b])
+        out.append((piv[q:q + s].astype(np.int64), Pall[p:p + s * c].reshape(s, c, order="F").copy()))
+        q += c
+        p += int(pmax[b]) * c
+    return out
+
+
 class Plan:
     """Device-resident CDS and task lists (``mxb_plan_*``).  ``pools`` optionally gives the
     numeric pools (D, B, VT) as CUDA tensors (e.g. from :func:`kernel_blocks`) instead of the

@@ -631,8 +631,12 @@ def _sample_rows(own: np.ndarray, cand: np.ndarray, nsamples: int, n: int,
 
 def build_cds(X: np.ndarray, kernel: KernelSpec, leaf_size: int = 256, budget: float = 0.03,
               tol: float = 1e-5, max_rank: int = 256, seed: int = 0,
-              neighbour_leaves: int = 4) -> CDS:
-    """Build the CDS of the kernel matrix of point set X (N x d, row-major)."""
+              neighbour_leaves: int = 4, id_on_gpu: bool = False) -> CDS:
+    """Build the CDS of the kernel matrix of point set X (N x d, row-major).
+
+    ``id_on_gpu``: the sample matrices of each tree level are computed on the GPU
+    (``mxb_kernel_blocks``) and factored there in one launch (``mxb_batched_id``) instead of
+    one host ID per node; sampling and the tree stay on the host."""
     X = np.ascontiguousarray(X, dtype=np.float64)
     n = X.shape[0]
     tree = build_tree(X, leaf_size)
@@ -665,7 +669,7 @@ def build_cds(X: np.ndarray, kernel: KernelSpec, leaf_size: int = 256, budget: f
     skels: List[np.ndarray] = [np.zeros(0, np.int64)] * nn
     proj: List[np.ndarray] = [np.zeros((0, 0))] * nn
 
-    def compress(v: int):
+    def prepare(v: int):
         own = tree.lids[v]
         if lch[v] == -1:
             bmap = own
@@ -687,16 +691,33 @@ def build_cds(X: np.ndarray, kernel: KernelSpec, leaf_size: int = 256, budget: f
             keep = merged[: 4 * leaf_size]
         nsamples = max(2 * len(bmap), 2 * leaf_size)
         amap = _sample_rows(own, cv, nsamples, n, np.random.default_rng([seed, v]))
+        return v, amap, bmap, keep
+
+    def compress(v: int):
+        v, amap, bmap, keep = prepare(v)
         K = kernel_matrix(X, amap, bmap, kernel)
         piv, P = interpolative_decomposition(np.asfortranarray(K), tol, max_rank)
         return v, bmap[piv], P, keep
 
+    def compress_level_on_gpu(pool, nodes):
+        from . import hgemm as H
+        prep = list(pool.map(prepare, nodes))
+        K, _ = H.kernel_matrices(dX, kernel, [q[1] for q in prep], [q[2] for q in prep])
+        ids = H.batched_id(K, [(len(q[1]), len(q[2])) for q in prep], tol, max_rank)
+        del K
+        return [(v, bmap[piv], P, keep) for (v, _, bmap, keep), (piv, P) in zip(prep, ids)]
+
+    dX = None
+    if id_on_gpu:
+        import torch
+        dX = torch.as_tensor(X).to("cuda")
     # nodes of one level are independent: LAPACK / BLAS release the GIL, so a thread pool
     # over the level with single-threaded BLAS inside scales with the host cores
     with _blas_single_thread(), ThreadPoolExecutor(max_workers=_workers()) as pool:
         for lev in range(tree.depth, 0, -1):
             nodes = list(range((1 << lev) - 1, (1 << (lev + 1)) - 1))
-            for v, sk, P, keep in pool.map(compress, nodes):
+            level = compress_level_on_gpu(pool, nodes) if id_on_gpu else pool.map(compress, nodes)
+            for v, sk, P, keep in level:
                 skels[v] = sk
                 proj[v] = P
                 slen[v] = P.shape[0]
