@@ -24,7 +24,6 @@
 namespace mxb {
 namespace {
 
-constexpr int THREADS = 256, WARPS = THREADS / 32;
 constexpr int MAX_COLS = 8192;  // shared memory holds 20 bytes per column
 
 struct IdJob {
@@ -42,8 +41,10 @@ __device__ __forceinline__ double warp_sum(double v)
 }
 
 // Sum over the block; every thread gets the result.  `red` holds WARPS + 1 doubles.
+template <int THREADS>
 __device__ double block_sum(double v, double *red)
 {
+    constexpr int WARPS = THREADS / 32;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     v = warp_sum(v);
     if (lane == 0) red[warp] = v;
@@ -60,8 +61,10 @@ __device__ double block_sum(double v, double *red)
 }
 
 // First index of the largest value in x[lo, hi); every thread gets it.
+template <int THREADS>
 __device__ int block_argmax(const double *x, int lo, int hi, double *redv, int *redi)
 {
+    constexpr int WARPS = THREADS / 32;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double bv = -1.0;
     int bi = hi;
@@ -98,11 +101,15 @@ __device__ int block_argmax(const double *x, int lo, int hi, double *redv, int *
     return r;
 }
 
+// THREADS: 256 when the launch has enough nodes to fill the GPU, 1024 (more warps on the
+// trailing columns of one node) when it has fewer nodes than SMs.
+template <int THREADS>
 __global__ void __launch_bounds__(THREADS) id_qrcp_kernel(const IdJob *__restrict__ jobs, double *__restrict__ A,
                                                           double *__restrict__ P, double *__restrict__ Z,
                                                           int32_t *__restrict__ piv, int32_t *__restrict__ rank,
                                                           double tol, int max_rank)
 {
+    constexpr int WARPS = THREADS / 32;
     extern __shared__ double sm[];
     __shared__ double red[WARPS + 1];
     __shared__ int redi[WARPS + 1];
@@ -133,7 +140,7 @@ __global__ void __launch_bounds__(THREADS) id_qrcp_kernel(const IdJob *__restric
     double r00 = 0.0;
     for (int i = 0; i < kmax; ++i) {
         if (i >= max_rank) break;  // s = max_rank
-        const int p = block_argmax(vn1, i, nc, red, redi);
+        const int p = block_argmax<THREADS>(vn1, i, nc, red, redi);
         if (p != i) {
             double *ci = a + (size_t)i * ns, *cp = a + (size_t)p * ns;
             for (int r = threadIdx.x; r < ns; r += THREADS) {
@@ -154,7 +161,7 @@ __global__ void __launch_bounds__(THREADS) id_qrcp_kernel(const IdJob *__restric
         double *ci = a + (size_t)i * ns;
         double x2 = 0.0;
         for (int r = i + 1 + threadIdx.x; r < ns; r += THREADS) x2 += ci[r] * ci[r];
-        x2 = block_sum(x2, red);
+        x2 = block_sum<THREADS>(x2, red);
         if (threadIdx.x == 0) {
             const double alpha = ci[i];
             const double xnorm = sqrt(x2);
@@ -291,10 +298,18 @@ extern "C" int32_t mxb_batched_id(double *dA, const int32_t *nrows, const int32_
     if (e == cudaSuccess) e = cudaMallocAsync(&dZ, std::max<uint64_t>(p, 1) * sizeof(double), s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dJobs, jobs.data(), jobs.size() * sizeof(IdJob), cudaMemcpyHostToDevice, s);
     const size_t smem = (size_t)maxc * (2 * sizeof(double) + sizeof(int));
+    int dev = 0, sms = 148;
+    if (e == cudaSuccess) e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const bool wide = count < sms;
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(id_qrcp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = wide ? cudaFuncSetAttribute(id_qrcp_kernel<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                 : cudaFuncSetAttribute(id_qrcp_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess) {
-        id_qrcp_kernel<<<(unsigned)count, THREADS, smem, s>>>(dJobs, dA, dP, dZ, dPiv, dRank, tol, max_rank);
+        if (wide)
+            id_qrcp_kernel<1024><<<(unsigned)count, 1024, smem, s>>>(dJobs, dA, dP, dZ, dPiv, dRank, tol, max_rank);
+        else
+            id_qrcp_kernel<256><<<(unsigned)count, 256, smem, s>>>(dJobs, dA, dP, dZ, dPiv, dRank, tol, max_rank);
         e = cudaGetLastError();
     }
     if (dJobs) cudaFreeAsync(dJobs, s);
