@@ -342,8 +342,8 @@ MXB_API int32_t mxb_kernel_blocks(const double *dX, int64_t n, int32_t d, int32_
  * and P_b (s_b x ncols[b]) with R11 P_b[:, piv] = R[0:s_b, :].  Outputs (device arrays):
  * dRank[b] = s_b; dPiv holds ncols[b] pivots per matrix, packed (the first s_b are the
  * skeleton columns); dP holds min(max_rank, ncols[b]) x ncols[b] doubles per matrix, packed,
- * of which the first s_b x ncols[b] are P_b (column-major, leading dimension s_b).
- * ncols <= 8192.  Asynchronous on `stream`. */
+ * of which the first s_b x ncols[b] are P_b (column-major, leading dimension s_b).  A zero
+ * matrix gets P_b = 0, as in the reference.  ncols <= 8192.  Asynchronous on `stream`. */
 MXB_API int32_t mxb_batched_id(double *dA, const int32_t *nrows, const int32_t *ncols, int32_t count,
                                double tol, int32_t max_rank, int32_t *dRank, int32_t *dPiv, double *dP,
                                void *stream);

@@ -11,7 +11,8 @@
 //   2. The reference's rank rule: s is the first s >= 1 with |R[s,s] / R[0,0]| < tol, at most
 //      max_rank and at most min(nrows, ncols).  The QR stops there: only R[0:s, :] is needed.
 //   3. P (s x ncols) with R11 P[:, piv] = R[0:s, :] by back substitution (upper triangular
-//      R11), columns in parallel.  If R[0,0] == 0, P has a 1 at (k, piv[k]) for k < s.
+//      R11), columns in parallel.  If R[0,0] == 0 (a zero matrix), P = 0: the reference then
+//      returns R's upper rows, which are zero, without the solve.
 // The factorisation is a sequence of rank-1 steps over the trailing matrix, each bound by
 // the memory traffic of that matrix (L2 for a few nodes in flight, HBM beyond).
 #include <cfloat>
@@ -234,8 +235,6 @@ __global__ void __launch_bounds__(THREADS) id_qrcp_kernel(const IdJob *__restric
     double *pout = P + jb.p_off;  // s x nc, leading dimension s
     if (r00 == 0.0) {
         for (int e = threadIdx.x; e < s * nc; e += THREADS) pout[e] = 0.0;
-        __syncthreads();
-        for (int k = threadIdx.x; k < s; k += THREADS) pout[k + (size_t)jp[k] * s] = 1.0;
         return;
     }
     // z[k][j] (row-major, j fastest: coalesced across the threads) = R[k, j]

@@ -409,7 +409,8 @@ def interpolative_decomposition(A: np.ndarray, tol: float, max_rank: int):
     """Column ID of A (rows = samples, cols = candidates), ``compression.h:446-523``.
 
     Pivoted QR; the rank s is the first s >= 1 with |R[s,s] / R[0,0]| < tol, capped at
-    max_rank; the projection P (s x ncols) solves R11 P[:, piv] = R[:s, :].
+    max_rank; the projection P (s x ncols) solves R11 P[:, piv] = R[:s, :].  A zero matrix
+    (R[0,0] == 0) gets P = 0, as the reference returns R's (zero) upper rows unsolved there.
     Returns (skeleton column positions, P).
     """
     ncols = A.shape[1]
@@ -425,9 +426,7 @@ def interpolative_decomposition(A: np.ndarray, tol: float, max_rank: int):
         s += 1
     s = min(s, max_rank, ncols)
     if r00 == 0:
-        P = np.zeros((s, ncols))
-        P[np.arange(s), piv[:s]] = 1.0
-        return piv[:s].copy(), P
+        return piv[:s].copy(), np.zeros((s, ncols))
     T = _sla.solve_triangular(R[:s, :s], R[:s, :], lower=False, check_finite=False)
     P = np.empty((s, ncols))
     P[:, piv] = T

@@ -74,6 +74,29 @@ def ref():
     return _ref
 
 
+def ref_decomposition(A: np.ndarray, tol: float):
+    """The reference's own column ID, ``decomposition`` (matroxTest-V1/compression.h:446-523:
+    dgeqp3, the rank rule with its maximum rank of 256 as written there, dtrsm), of A
+    (nrows > ncols).  Returns (skeleton columns, P) like
+    ``structure.interpolative_decomposition``."""
+    lib = ref()
+    a = np.array(A, dtype=np.float64, order="F", copy=True)
+    nr, nc = a.shape
+    sk = ctypes.POINTER(ctypes.c_int)()
+    pr = ctypes.POINTER(ctypes.c_double)()
+    jp = ctypes.POINTER(ctypes.c_int)()
+    lib.ref_decomposition.restype = ctypes.c_int
+    lib.ref_decomposition.argtypes = [_P, ctypes.c_int, ctypes.c_int, ctypes.c_double, _P, _P, _P]
+    s = lib.ref_decomposition(a.ctypes.data_as(_P), nr, nc, tol, ctypes.byref(sk), ctypes.byref(pr),
+                              ctypes.byref(jp))
+    skels = np.ctypeslib.as_array(sk, shape=(s,)).astype(np.int64).copy()
+    P = np.ctypeslib.as_array(pr, shape=(s * nc,)).reshape(s, nc, order="F").copy()
+    lib.ref_id_free.argtypes = [_P]
+    for q in (sk, pr, jp):
+        lib.ref_id_free(ctypes.cast(q, _P))
+    return skels, P
+
+
 class Workspace:
     """Host arrays of one evaluation in the reference's layout for a given nrhs."""
 

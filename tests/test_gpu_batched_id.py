@@ -57,7 +57,8 @@ def test_batched_id_matches_host_id(torch, tol, max_rank):
             err = np.linalg.norm(m[:, piv] @ P - m) / np.linalg.norm(m)
             assert err <= 100 * tol + 1e-12, (b, err)
     ranks = [len(p) for p, _ in got]
-    assert ranks[5] == 5 and ranks[6] == min(12, max_rank)  # exact rank 5; zero matrix: identity
+    assert ranks[5] == 5 and ranks[6] == min(12, max_rank)  # exact rank 5; zero matrix: full
+    assert not got[6][1].any()  # zero matrix: P = 0, as in the reference
     if max_rank == 40:
         assert ranks[1] == 40  # capped
 
