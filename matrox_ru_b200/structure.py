@@ -630,17 +630,26 @@ def _sample_rows(own: np.ndarray, cand: np.ndarray, nsamples: int, n: int,
 
 def build_cds(X: np.ndarray, kernel: KernelSpec, leaf_size: int = 256, budget: float = 0.03,
               tol: float = 1e-5, max_rank: int = 256, seed: int = 0,
-              neighbour_leaves: int = 4, id_on_gpu: bool = False) -> CDS:
+              neighbour_leaves: int = 4, id_on_gpu: bool = False, structure=None) -> CDS:
     """Build the CDS of the kernel matrix of point set X (N x d, row-major).
 
     ``id_on_gpu``: the sample matrices of each tree level are computed on the GPU
     (``mxb_kernel_blocks``) and factored there in one launch (``mxb_batched_id``) instead of
-    one host ID per node; sampling and the tree stay on the host."""
+    one host ID per node; sampling and the tree stay on the host.
+
+    ``structure``: a :class:`~matrox_ru_b200.structure_bin.Structure` (tree, near and far
+    lists), e.g. read from the reference's ``.bin`` files, used instead of building one;
+    ``budget`` is then unused and ``leaf_size`` only sizes the samples."""
     X = np.ascontiguousarray(X, dtype=np.float64)
     n = X.shape[0]
-    tree = build_tree(X, leaf_size)
-    near = near_lists(tree, budget)
-    far = far_lists(tree, near)
+    if structure is None:
+        tree = build_tree(X, leaf_size)
+        near = near_lists(tree, budget)
+        far = far_lists(tree, near)
+    else:
+        tree, near, far = structure.tree, structure.near, structure.far
+        if sum(len(tree.lids[tree.leaf_node(i)]) for i in range(tree.nleaf)) != n:
+            raise ValueError("the structure's leaves do not hold the N points of X")
     is_hss = all(len(l) == 1 for l in near)
     nn = tree.numnodes
 
