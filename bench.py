@@ -646,6 +646,8 @@ def main():
                   "nodes_same_rank": float(np.mean([cds.slen[v] == cg.slen[v] for v in nodes])),
                   "nodes_same_skeleton": float(np.mean([np.array_equal(np.sort(cds.skels[v]), np.sort(cg.skels[v]))
                                                         for v in nodes]))}
+        if cg.VT.shape == cds.VT.shape and cds.VT.size:  # the projections: GPU ID vs host ID
+            gpu_id["max_rel_diff_VT_vs_host_build"] = float(np.abs(cg.VT - cds.VT).max() / np.abs(cds.VT).max())
         del cg
         torch.cuda.empty_cache()
     launches = head["launches_per_eval"] * args.steps
