@@ -1,4 +1,4 @@
-"""GPU: batches of uneven H-matrices (scaled down): different N, point
+"""GPU: batches of uneven H-matrices (the 64-matrix batch workload, scaled down): different N, point
 dimension, kernel (Gaussian / inverse multiquadric), ranks and nrhs, evaluated by one merged
 launch sequence with autotuned column tiles; each result is checked against the FP64 oracle."""
 import numpy as np
@@ -77,7 +77,7 @@ def test_batch_accumulates(torch):
 
 
 def c3_like_cases(count, seed):
-    """BASELINE config 3's recipe with N scaled down: N log-uniform, d from {8, 18, 28, 54},
+    """The batch workload's recipe with N scaled down: N log-uniform, d from {8, 18, 28, 54},
     Gaussian (h in [0.5, 3]) or inverse multiquadric kernels, nrhs log-uniform in [32, 512]."""
     rng = np.random.default_rng(seed)
     out = []

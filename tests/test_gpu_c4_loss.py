@@ -1,4 +1,4 @@
-"""GPU: the differentiable kernel-ridge loss L = 0.5 ||K~ W - Y||^2 on an
+"""GPU: the differentiable kernel-ridge loss L = 0.5 ||K~ W - Y||^2 (N = 262144 workload) on an
 N = 8192 subsample of its point distribution (d = 18, 32 components, Gaussian h = 1.5,
 H2-b budget 0.03, ID tolerance 1e-5, 64 columns, W and Y FP32).  The gradient from the
 transposed traversal is checked against central finite differences (exact for a quadratic
