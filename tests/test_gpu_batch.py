@@ -76,7 +76,7 @@ def test_batch_accumulates(torch):
         assert np.linalg.norm(o.cpu().numpy() - want) / np.linalg.norm(want) <= 1e-5
 
 
-def c3_like_cases(count, seed):
+def uneven_batch_cases(count, seed):
     """The batch workload's recipe with N scaled down: N log-uniform, d from {8, 18, 28, 54},
     Gaussian (h in [0.5, 3]) or inverse multiquadric kernels, nrhs log-uniform in [32, 512]."""
     rng = np.random.default_rng(seed)
@@ -94,7 +94,7 @@ def c3_like_cases(count, seed):
 
 
 def test_sixty_four_uneven_matrices_one_sequence(torch):
-    cases = c3_like_cases(64, seed=9)
+    cases = uneven_batch_cases(64, seed=9)
     plans = [H.Plan(c, "split_bf16") for c, _ in cases]
     batch = H.Batch(plans)
     per_plan = max(p.info()["launches"] for p in plans)

@@ -1,4 +1,4 @@
-"""GPU: the full c1 workload (H2-b, N=65536, d=28, 1024 rhs) through size-independent
+"""GPU: the full H2-b workload (N=65536, d=28, 1024 rhs) through size-independent
 properties and a column slice of the reference's own evaluator."""
 import numpy as np
 import pytest
@@ -20,7 +20,7 @@ def torch():
 
 
 @pytest.fixture(scope="module")
-def c1():
+def h2b_65536():
     X = S.gaussian_mixture(65536, 28, 16, -2.0, 2.0, 0.3, 1.0, seed=SEED)
     return S.build_cds(X, S.KernelSpec("gaussian", 2.0), leaf_size=256, budget=0.03, tol=1e-5,
                        max_rank=256, seed=SEED)
@@ -34,17 +34,17 @@ def leaf_slice(cds, TW, r_full, r):
     return out
 
 
-def test_c1_structure_matches_reference_scale(c1):
-    assert (c1.nleaf, c1.ncount) == (256, 1536) and 2900 <= c1.fcount <= 3400
-    assert 8.0e11 <= c1.flops(1024) <= 9.0e11  # the reference's c1-shaped probe: 8.12e11
+def test_h2b_65536_structure_matches_reference_scale(h2b_65536):
+    assert (h2b_65536.nleaf, h2b_65536.ncount) == (256, 1536) and 2900 <= h2b_65536.fcount <= 3400
+    assert 8.0e11 <= h2b_65536.flops(1024) <= 9.0e11  # the reference's probe at this shape: 8.12e11
 
 
-def test_c1_fp64_reference_slice_linearity_and_adjoint(torch, c1):
+def test_h2b_65536_fp64_reference_slice_linearity_and_adjoint(torch, h2b_65536):
     r = 1024
     rng = np.random.default_rng(1)
-    W1 = torch.as_tensor(rng.standard_normal(c1.n * r), device="cuda")
-    W2 = torch.as_tensor(rng.standard_normal(c1.n * r), device="cuda")
-    plan = H.Plan(c1, "fp64")
+    W1 = torch.as_tensor(rng.standard_normal(h2b_65536.n * r), device="cuda")
+    W2 = torch.as_tensor(rng.standard_normal(h2b_65536.n * r), device="cuda")
+    plan = H.Plan(h2b_65536, "fp64")
     Y1 = plan.evaluate(W1, r)
     Y2 = plan.evaluate(W2, r)
     Y12 = plan.evaluate(2.0 * W1 - 0.5 * W2, r)
@@ -53,12 +53,12 @@ def test_c1_fp64_reference_slice_linearity_and_adjoint(torch, c1):
     # the reference's CBHGEMM on the first 8 columns of every leaf block
     if O.ref_available():
         rs = 8
-        tw = leaf_slice(c1, W1.cpu().numpy(), r, rs)
-        want = O.eval_h2b(c1, tw, rs, use_reference=True)
-        got = leaf_slice(c1, Y1.cpu().numpy(), r, rs)
+        tw = leaf_slice(h2b_65536, W1.cpu().numpy(), r, rs)
+        want = O.eval_h2b(h2b_65536, tw, rs, use_reference=True)
+        got = leaf_slice(h2b_65536, Y1.cpu().numpy(), r, rs)
         assert np.abs(got - want).max() / np.abs(want).max() <= 1e-12
     # adjoint identity <K~ W, G> = <W, K~^T G> at full size
-    G = torch.as_tensor(rng.standard_normal(c1.n * r), device="cuda")
+    G = torch.as_tensor(rng.standard_normal(h2b_65536.n * r), device="cuda")
     A = plan.adjoint(G, r)
     lhs = torch.dot(Y1, G).item()
     rhs = torch.dot(W1, A).item()
@@ -66,35 +66,35 @@ def test_c1_fp64_reference_slice_linearity_and_adjoint(torch, c1):
 
 
 @pytest.mark.parametrize("mode,tol", [("split_bf16", 1e-5), ("split_bf16_x6", 4e-6)])
-def test_c1_split_bf16_full_columns(torch, c1, mode, tol):
+def test_h2b_65536_split_bf16_full_columns(torch, h2b_65536, mode, tol):
     r = 1024
-    W = torch.as_tensor(np.random.default_rng(2).standard_normal(c1.n * r), device="cuda")
-    want = H.Plan(c1, "fp64").evaluate(W, r)
-    plan = H.Plan(c1, mode)
+    W = torch.as_tensor(np.random.default_rng(2).standard_normal(h2b_65536.n * r), device="cuda")
+    want = H.Plan(h2b_65536, "fp64").evaluate(W, r)
+    plan = H.Plan(h2b_65536, mode)
     got = plan.evaluate(W, r)
     plan.status()
     err = (torch.linalg.norm(got - want) / torch.linalg.norm(want)).item()
     assert 1e-12 < err <= tol, err
 
 
-def test_c1_split_dropin_first_call(torch, c1):
+def test_h2b_65536_split_dropin_first_call(torch, h2b_65536):
     """The first drop-in call creates the evaluation graphs of its slab buffers while earlier
     slabs are in flight and the PCIe bus is busy with slab copies: every slab of that call
     must match the plan API on all 1024 columns (the graphs' tables are uploaded in stream
     order, ahead of the launches that read them)."""
     r = 1024
-    W = torch.as_tensor(np.random.default_rng(3).standard_normal(c1.n * r), device="cuda")
-    want = H.Plan(c1, "split_bf16").evaluate(W, r).cpu().numpy()
-    tw = torch.empty(c1.n * r, dtype=torch.float64, pin_memory=True)
+    W = torch.as_tensor(np.random.default_rng(3).standard_normal(h2b_65536.n * r), device="cuda")
+    want = H.Plan(h2b_65536, "split_bf16").evaluate(W, r).cpu().numpy()
+    tw = torch.empty(h2b_65536.n * r, dtype=torch.float64, pin_memory=True)
     tw.copy_(W.cpu())
-    y = torch.zeros(c1.n * r, dtype=torch.float64, pin_memory=True)
+    y = torch.zeros(h2b_65536.n * r, dtype=torch.float64, pin_memory=True)
     H.cache_invalidate()
     H.set_precision("split_bf16")
     try:
         for flags in (_lib.FLAG_OUTPUT_IS_ZERO, 0):
             H.set_flags(flags)
             y.zero_()
-            H.evaluate_host(c1, tw.numpy(), r, apres=y.numpy())
+            H.evaluate_host(h2b_65536, tw.numpy(), r, apres=y.numpy())
             got = y.numpy()
             assert np.abs(got - want).max() <= 1e-6 * np.abs(want).max(), flags
     finally:
@@ -104,7 +104,7 @@ def test_c1_split_dropin_first_call(torch, c1):
 
 
 @pytest.fixture(scope="module")
-def hss_c0():
+def hss_16384():
     """HSS (near-field budget 0): N = 16384 points in d = 8 from an 8-component isotropic
     mixture (means uniform in [0, 4]^8, sigma 0.5), Gaussian h = 1, leaf 128, ID tolerance
     1e-5, max rank 128."""
@@ -113,11 +113,11 @@ def hss_c0():
     return X, spec, S.build_cds(X, spec, leaf_size=128, budget=0.0, tol=1e-5, max_rank=128, seed=SEED)
 
 
-def test_hss_full_size_vs_reference(torch, hss_c0):
+def test_hss_full_size_vs_reference(torch, hss_16384):
     """The HSS drop-in on all 256 columns against the reference's own parHSSGEMM (FP64,
     <= 1e-12), the split-BF16 path against FP64 (<= 1e-5), and both against the dense K W
     on sampled rows (the compression error, the same for both)."""
-    X, spec, cds = hss_c0
+    X, spec, cds = hss_16384
     assert cds.is_hss and cds.nleaf == 128
     r = 256
     TW = np.random.default_rng(8).standard_normal(cds.n * r)

@@ -30,7 +30,7 @@ def problem():
     return X, spec, cds
 
 
-def test_c4_gradient_fd_and_dense(torch, problem):
+def test_loss_gradient_fd_and_dense(torch, problem):
     X, spec, cds = problem
     ev = H.Evaluator(cds)
     r = 64

@@ -11,7 +11,7 @@
   d = 18 (32-component mixture, Gaussian h = 1.5, budget 0.03, tolerance 1e-5), W and Y
   262144 x 64 FP32: the gradient from the transposed traversal agrees with central finite
   differences to 1e-6 relative and satisfies <K~ W, G> = <W, K~^T G>.  (The dense K^T G
-  check runs on an N = 8192 subsample in test_gpu_c4_loss.py.)
+  check runs on an N = 8192 subsample in test_gpu_loss_gradient.py.)
 """
 import numpy as np
 import pytest

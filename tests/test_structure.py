@@ -96,10 +96,10 @@ def test_save_load_roundtrip(tmp_path, small_cases):
     cds = small_cases["h2b"]
     p = tmp_path / "c.npz"
     cds.save(str(p))
-    c2 = S.CDS.load(str(p))
+    back = S.CDS.load(str(p))
     for k in S.CDS._ARRAYS:
-        assert np.array_equal(getattr(cds, k), getattr(c2, k)), k
-    assert (c2.n, c2.nleaf, c2.numnodes, c2.is_hss) == (cds.n, cds.nleaf, cds.numnodes, cds.is_hss)
+        assert np.array_equal(getattr(cds, k), getattr(back, k)), k
+    assert (back.n, back.nleaf, back.numnodes, back.is_hss) == (cds.n, cds.nleaf, cds.numnodes, cds.is_hss)
 
 
 def test_offsets_match_reference_layout(small_cases):
