@@ -81,3 +81,20 @@ def test_reader_rejects_bad_structures(tmp_path):
     os.remove(tmp_path / "dim.bin")
     with pytest.raises(FileNotFoundError):
         B.read_structure(str(tmp_path), X)
+
+
+def test_nn_lists_round_trip(tmp_path):
+    """NN.bin (int32) and distNN.bin (float64, one distance per NN entry) as the reference's
+    reader expects them (matroxTest-V1/HTree.h:78-94)."""
+    X, sargs, _ = case("hss")
+    st = B.build_structure(X, **sargs)
+    k = 4
+    d2 = S.sqdist(X, X)
+    np.fill_diagonal(d2, np.inf)
+    nn = np.argsort(d2, axis=1, kind="stable")[:, :k]
+    st.NN = nn.reshape(-1)
+    st.distNN = np.sqrt(np.take_along_axis(d2, nn, axis=1)).reshape(-1)
+    B.write_structure(st, str(tmp_path))
+    assert os.path.getsize(tmp_path / "distNN.bin") == 2 * os.path.getsize(tmp_path / "NN.bin")
+    rd = B.read_structure(str(tmp_path), X)
+    assert np.array_equal(rd.NN, st.NN) and np.array_equal(rd.distNN, st.distNN)
