@@ -66,8 +66,21 @@ MXB_API const char *mxb_version(void);
 /* Precision used by the drop-ins (default MXB_PREC_FP64). */
 MXB_API int32_t mxb_set_precision(int32_t mode);
 MXB_API int32_t mxb_set_flags(uint32_t flags);
-/* Drop every cached device copy of a CDS (required after changing CDS values in place). */
+/* Drop every cached device copy of a CDS.  Required, in the default mode, after changing CDS
+ * values in place AND after freeing a CDS and allocating a new one that may land at the same
+ * addresses with the same sizes: the default key covers the pool pointers, every index array
+ * and about 4096 sampled values per pool, not every value. */
 MXB_API int32_t mxb_cache_invalidate(void);
+/* How the drop-ins recognise a CDS they have already uploaded (no counterpart in the
+ * reference, which reads the host CDS on every call).  Setting a mode drops the cache.
+ *   MXB_CACHE_SAMPLED (default): pointers, index arrays, ~4096 sampled values per pool.
+ *   MXB_CACHE_FULL: pointers, index arrays and every value of D, B and VT (a host pass over
+ *     the pools on every call, ~0.5 s per GB on one core; no invalidation needed).
+ *   MXB_CACHE_OFF: upload the CDS on every call, as the reference reads it on every call. */
+#define MXB_CACHE_SAMPLED 0
+#define MXB_CACHE_FULL 1
+#define MXB_CACHE_OFF 2
+MXB_API int32_t mxb_cache_set_mode(int32_t mode);
 
 /* ---- drop-ins: H2-b -------------------------------------------------------------------- */
 
@@ -356,14 +369,16 @@ MXB_API int32_t mxb_batched_id(double *dA, const int32_t *nrows, const int32_t *
  * the device -- this computes dY (+)= K~ dW in FP64 like mxb_plan_evaluate and allocates
  * nothing: `desc` carries HOST index arrays but DEVICE pointers in desc->D, desc->B and
  * desc->VT (with their lengths); dW and dY are device arrays in the packed leaf-blocked
- * layout.  Task lists, per-leaf offsets and skeleton workspaces live in one static device
+ * layout.  Pools, dW and dY that are not device memory of the current device (or managed
+ * memory) are rejected with MXB_ERR_ARG before anything is launched.  Task lists, per-leaf offsets and skeleton workspaces live in one static device
  * array of MXB_NOALLOC_SCRATCH_BYTES (32 MiB) that every GPU loading the library keeps until
  * exit; larger problems (skeleton rows x nrhs x 16 bytes plus the task lists) are rejected
  * with MXB_ERR_UNSUPPORTED.  The first call on a device looks the array's address up
- * (cudaGetSymbolAddress), so make it before any stream capture.  Every call shares the
- * array and overwrites all of it that it reads, so nothing needs clearing, but calls that
- * overlap on the GPU (other streams, other host threads) race on it.  Asynchronous on
- * `stream`. */
+ * (cudaGetSymbolAddress), so make it before any stream capture.  Each call copies its task
+ * lists from temporary host memory (pageable, so the copy may block the host), and returns
+ * MXB_ERR_UNSUPPORTED on a stream that is capturing.  Every call shares the array and
+ * overwrites all of it that it reads, so nothing needs clearing, but calls that overlap on
+ * the GPU (other streams, other host threads) race on it.  Asynchronous on `stream`. */
 #define MXB_NOALLOC_SCRATCH_BYTES (32u << 20)
 MXB_API int32_t mxb_evaluate_noalloc(const mxb_cds_desc *desc, const double *dW, double *dY, int32_t nrhs,
                                      int32_t accumulate, void *stream);

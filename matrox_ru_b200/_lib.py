@@ -19,6 +19,7 @@ MXB_ERR_CUDA = -3
 MXB_ERR_NOMEM = -4
 MXB_ERR_TIMEOUT = -5
 MXB_ERR_UNSUPPORTED = -6
+MXB_CACHE_SAMPLED, MXB_CACHE_FULL, MXB_CACHE_OFF = 0, 1, 2
 PREC_FP64 = 0
 PREC_SPLIT_BF16 = 1
 PREC_SPLIT_BF16_FAR6 = 2
@@ -89,6 +90,7 @@ def load(path: str = LIB_PATH):
             f.restype = I32
     lib.mxb_set_precision.argtypes = [I32]
     lib.mxb_set_flags.argtypes = [U32]
+    lib.mxb_cache_set_mode.argtypes = [I32]
     lib.mxb_plan_create.argtypes = [ctypes.POINTER(CdsDesc), I32, ctypes.POINTER(P)]
     lib.mxb_plan_destroy.argtypes = [P]
     lib.mxb_plan_evaluate.argtypes = [P, P, P, I32, P, P, I32, P]

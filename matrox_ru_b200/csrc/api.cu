@@ -77,15 +77,41 @@ uint64_t fnv_sample(uint64_t h, const double *p, uint64_t n)
     return fnv(h, p + n - 1, sizeof(double));
 }
 
+// every word of a numeric pool: four independent multiply-rotate lanes over 64-bit words
+uint64_t hash_full(uint64_t h, const double *p, uint64_t n)
+{
+    h = fnv(h, &n, sizeof(n));
+    if (!p || !n) return h;
+    const uint64_t *w = reinterpret_cast<const uint64_t *>(p);
+    uint64_t a[4] = {h, h ^ 0x9e3779b97f4a7c15ull, h ^ 0xc2b2ae3d27d4eb4full, h ^ 0x165667b19e3779f9ull};
+    uint64_t i = 0;
+    for (; i + 4 <= n; i += 4)
+        for (int k = 0; k < 4; ++k) {
+            a[k] ^= w[i + k];
+            a[k] *= 0x9fb21c651e98df25ull;
+            a[k] = (a[k] << 29) | (a[k] >> 35);
+        }
+    for (; i < n; ++i) a[0] = (a[0] ^ w[i]) * 0x9fb21c651e98df25ull;
+    return fnv(h, a, sizeof(a));
+}
+
+int g_cache_mode = MXB_CACHE_SAMPLED;
+
 uint64_t desc_key(const mxb_cds_desc &d)
 {
     uint64_t h = 1469598103934665603ull;
     const void *ptrs[] = {d.D, d.B, d.VT};
     h = fnv(h, ptrs, sizeof(ptrs));
     h = fnv(h, &d.nleaf, sizeof(int32_t) * 3);
-    h = fnv_sample(h, d.D, d.D_len);
-    h = fnv_sample(h, d.B, d.B_len);
-    h = fnv_sample(h, d.VT, d.VT_len);
+    if (g_cache_mode == MXB_CACHE_FULL) {
+        h = hash_full(h, d.D, d.D_len);
+        h = hash_full(h, d.B, d.B_len);
+        h = hash_full(h, d.VT, d.VT_len);
+    } else {
+        h = fnv_sample(h, d.D, d.D_len);
+        h = fnv_sample(h, d.B, d.B_len);
+        h = fnv_sample(h, d.VT, d.VT_len);
+    }
     h = fnv_arr(h, d.Dptr, d.ncount);
     h = fnv_arr(h, d.Bptr, d.fcount);
     h = fnv_arr(h, d.VTptr, d.numnodes);
@@ -105,6 +131,7 @@ int cached_plan(const mxb_cds_desc &d, Plan **out)
 {
     int dev = 0;
     API_CUDA(cudaGetDevice(&dev));
+    if (g_cache_mode == MXB_CACHE_OFF) g_cache.clear();
     const uint64_t key = desc_key(d);
     for (auto it = g_cache.begin(); it != g_cache.end(); ++it) {
         if (it->key == key && it->device == dev && it->precision == g_precision) {
@@ -532,6 +559,18 @@ int32_t mxb_set_flags(uint32_t flags)
 int32_t mxb_cache_invalidate(void)
 {
     std::lock_guard<std::mutex> lock(g_mu);
+    g_cache.clear();
+    return MXB_OK;
+}
+
+int32_t mxb_cache_set_mode(int32_t mode)
+{
+    if (mode != MXB_CACHE_SAMPLED && mode != MXB_CACHE_FULL && mode != MXB_CACHE_OFF) {
+        set_error("mxb_cache_set_mode: mode must be MXB_CACHE_SAMPLED, MXB_CACHE_FULL or MXB_CACHE_OFF");
+        return MXB_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lock(g_mu);
+    g_cache_mode = mode;
     g_cache.clear();
     return MXB_OK;
 }

@@ -57,6 +57,30 @@ int scratch_address(void **out)
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
+// The kernels read D, B, VT and W and write Y directly, so each must be memory of the current
+// device (or managed memory).  A host pointer here -- e.g. a descriptor built for
+// mxb_plan_create, whose pools are host arrays -- is rejected before anything is launched.
+int check_device_pointer(const void *ptr, const char *what)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    cudaPointerAttributes a{};
+    if (e == cudaSuccess) e = cudaPointerGetAttributes(&a, ptr);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_error(std::string("mxb_evaluate_noalloc: ") + what + ": cudaPointerGetAttributes: " +
+                  cudaGetErrorString(e));
+        return MXB_ERR_ARG;
+    }
+    const bool ok = a.type == cudaMemoryTypeManaged || (a.type == cudaMemoryTypeDevice && a.device == dev);
+    if (!ok) {
+        set_error(std::string("mxb_evaluate_noalloc: ") + what + " must be device memory of the current device "
+                  "(this entry point reads the CDS pools, W and Y in place)");
+        return MXB_ERR_ARG;
+    }
+    return MXB_OK;
+}
+
 }  // namespace
 }  // namespace mxb
 
@@ -69,9 +93,30 @@ extern "C" int32_t mxb_evaluate_noalloc(const mxb_cds_desc *desc, const double *
         set_error("mxb_evaluate_noalloc: null argument or nrhs < 1");
         return MXB_ERR_ARG;
     }
+    cudaStream_t s = (cudaStream_t)stream;
+    // The task lists are staged from host vectors that this call frees on return; a capturing
+    // stream would record copies that read them after they are gone.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaError_t ce = cudaStreamIsCapturing(s, &cap);
+    if (ce != cudaSuccess) {
+        cudaGetLastError();
+        set_error(std::string("mxb_evaluate_noalloc: cudaStreamIsCapturing: ") + cudaGetErrorString(ce));
+        return MXB_ERR_CUDA;
+    }
+    if (cap != cudaStreamCaptureStatusNone) {
+        set_error("mxb_evaluate_noalloc: the stream is capturing; this entry point copies each call's task lists "
+                  "from temporary host memory and is called outside stream capture");
+        return MXB_ERR_UNSUPPORTED;
+    }
+    int rc = MXB_OK;
+    if (desc->D_len && (rc = check_device_pointer(desc->D, "desc->D"))) return rc;
+    if (desc->B_len && (rc = check_device_pointer(desc->B, "desc->B"))) return rc;
+    if (desc->VT_len && (rc = check_device_pointer(desc->VT, "desc->VT"))) return rc;
+    if ((rc = check_device_pointer(dW, "dW"))) return rc;
+    if ((rc = check_device_pointer(dY, "dY"))) return rc;
     // host-side structure and task lists only: this Plan never touches device memory
     Plan p;
-    int rc = p.validate(*desc);
+    rc = p.validate(*desc);
     if (rc) return rc;
     p.build_tasks(row_tile_for(MXB_PREC_FP64));
 
@@ -104,8 +149,8 @@ extern "C" int32_t mxb_evaluate_noalloc(const mxb_cds_desc *desc, const double *
     rc = scratch_address(&base);
     if (rc) return rc;
     unsigned char *b = static_cast<unsigned char *>(base);
-    cudaStream_t s = (cudaStream_t)stream;
-    // pageable sources: each copy has consumed its host buffer when the call returns
+    // pageable sources: each copy has consumed its host buffer when the call returns (the
+    // copies may therefore block the host until the stream reaches them)
     cudaError_t e = cudaSuccess;
     if (tasks_b) e = cudaMemcpyAsync(b, p.tasks.data(), tasks_b, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess && items_b) e = cudaMemcpyAsync(b + off_items, p.items.data(), items_b, cudaMemcpyHostToDevice, s);

@@ -52,6 +52,14 @@ def cache_invalidate() -> None:
     check(_lib.load().mxb_cache_invalidate(), "mxb_cache_invalidate")
 
 
+CACHE_MODES = {"sampled": _lib.MXB_CACHE_SAMPLED, "full": _lib.MXB_CACHE_FULL, "off": _lib.MXB_CACHE_OFF}
+
+
+def cache_set_mode(mode: str) -> None:
+    """How the drop-ins recognise an uploaded CDS: "sampled" (default), "full" or "off"."""
+    check(_lib.load().mxb_cache_set_mode(CACHE_MODES[mode]), "mxb_cache_set_mode")
+
+
 def _ref_args(cds, TW, apres, nrhs, wskel, uskel, idx):
     a = _Args()
     wptr, uptr, wsko, usko, _ = cds.offsets(nrhs)

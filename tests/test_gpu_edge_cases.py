@@ -59,3 +59,27 @@ def test_split_extreme_nrhs(torch, small_cases, nrhs):
     got = plan.evaluate(torch.as_tensor(TW, device="cuda"), nrhs).cpu().numpy()
     plan.status()
     assert 1e-12 < np.linalg.norm(got - want) / np.linalg.norm(want) <= 1e-5
+
+
+def test_dropin_cache_modes_see_in_place_edits(torch, small_cases):
+    """The drop-ins cache the uploaded CDS.  An in-place edit of a value that the default
+    (sampled) key does not read is seen after mxb_cache_invalidate, and at once in the
+    "full" (every value hashed) and "off" (upload every call) modes."""
+    cds = small_cases["h2b"]
+    assert cds.D.size >= 2 * 4096  # so the sampled key skips some values
+    r = 6
+    TW = np.random.default_rng(5).standard_normal(cds.n * r)
+    D0 = cds.D.copy()
+    try:
+        for mode in ("full", "off", "sampled"):
+            H.cache_set_mode(mode)
+            cds.D[:] = D0
+            assert rel_err(H.evaluate_host(cds, TW, r), O.eval_h2b(cds, TW, r)) <= 1e-12
+            cds.D[1] += 0.5  # in place: same pointer, same length
+            want = O.eval_h2b(cds, TW, r)
+            if mode == "sampled":
+                H.cache_invalidate()
+            assert rel_err(H.evaluate_host(cds, TW, r), want) <= 1e-12, mode
+    finally:
+        cds.D[:] = D0
+        H.cache_set_mode("sampled")

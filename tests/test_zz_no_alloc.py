@@ -84,3 +84,54 @@ def test_noalloc_rejects_problems_beyond_the_static_scratch(torch):
                                   torch.cuda.current_stream().cuda_stream)
     assert rc == _lib.MXB_ERR_UNSUPPORTED
     assert b"MXB_NOALLOC_SCRATCH_BYTES" in lib.mxb_last_error()
+
+
+def test_noalloc_rejects_host_pools(torch):
+    """A descriptor whose pools are host arrays (as mxb_plan_create accepts) is refused with
+    MXB_ERR_ARG before anything is launched."""
+    lib = _lib.load()
+    name, cds = next(_cases())
+    keep = []
+    desc = H.cds_desc(cds, keep)  # D / B / VT left as host arrays
+    r = 4
+    W = torch.zeros(cds.n * r, dtype=torch.float64, device="cuda")
+    Y = torch.zeros_like(W)
+    rc = lib.mxb_evaluate_noalloc(ctypes.byref(desc), W.data_ptr(), Y.data_ptr(), r, 0,
+                                  torch.cuda.current_stream().cuda_stream)
+    assert rc == _lib.MXB_ERR_ARG
+    assert b"device memory" in lib.mxb_last_error()
+    # host W with device pools is refused the same way
+    keep2 = []
+    ddesc = _device_desc(torch, cds, keep2)
+    Wh = np.zeros(cds.n * r)
+    rc = lib.mxb_evaluate_noalloc(ctypes.byref(ddesc), Wh.ctypes.data, Y.data_ptr(), r, 0,
+                                  torch.cuda.current_stream().cuda_stream)
+    assert rc == _lib.MXB_ERR_ARG
+    torch.cuda.synchronize()
+
+
+def test_noalloc_refuses_a_capturing_stream(torch):
+    """Each call copies its task lists from temporary host memory, so a capturing stream is
+    refused with MXB_ERR_UNSUPPORTED (nothing is enqueued) instead of recording copies that
+    would read freed host memory on replay."""
+    lib = _lib.load()
+    name, cds = next(_cases())
+    keep = []
+    desc = _device_desc(torch, cds, keep)
+    r = 4
+    W = torch.zeros(cds.n * r, dtype=torch.float64, device="cuda")
+    Y = torch.zeros_like(W)
+    side = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(side):
+        g.capture_begin()
+        try:
+            rc = lib.mxb_evaluate_noalloc(ctypes.byref(desc), W.data_ptr(), Y.data_ptr(), r, 0,
+                                          side.cuda_stream)
+            Y.add_(1.0)  # keeps the captured graph non-empty
+        finally:
+            g.capture_end()
+    assert rc == _lib.MXB_ERR_UNSUPPORTED
+    assert b"capturing" in lib.mxb_last_error()
+    del g
+    torch.cuda.synchronize()
