@@ -1,4 +1,4 @@
-"""Generates the reference-pipeline fixtures of tests/golden (``ref_pipeline_*.npz``).
+"""Generates the reference-pipeline fixtures ``tests/golden/ref_pipeline/*.npz``.
 
 Unlike ``make_golden.py``, whose CDSs come from this repository's producer, these fixtures
 hold a CDS made end to end by the REFERENCE's own host code, built from its sources by
@@ -37,8 +37,8 @@ import ref_pipeline as RP  # noqa: E402
 
 CASES = {
     # name: (n, d, components, mean_lo, mean_hi, sigma, seed, budget, leaf, tol, h, max_rank, nrhs)
-    "ref_pipeline_hss_n1024": (1024, 8, 8, 0.0, 4.0, 0.5, 201, 0.0, 32, 1e-5, 1.0, 24, 5),
-    "ref_pipeline_h2b_n1024": (1024, 8, 8, 0.0, 4.0, 0.5, 202, 0.12, 32, 1e-5, 1.0, 24, 4),
+    "hss_n1024": (1024, 8, 8, 0.0, 4.0, 0.5, 201, 0.0, 32, 1e-5, 1.0, 24, 5),
+    "h2b_n1024": (1024, 8, 8, 0.0, 4.0, 0.5, 202, 0.12, 32, 1e-5, 1.0, 24, 4),
 }
 
 # One C++ translation unit around the generated evaluator: the generated header defines
@@ -101,7 +101,8 @@ def main():
     ref_root = sys.argv[1]
     if not (RP.available() and O.ref_available()):
         raise SystemExit("oracle/_ref is not built: make -C oracle REF_ROOT=<reference tree>")
-    out_dir = os.path.dirname(os.path.abspath(__file__))
+    out_dir = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ref_pipeline")
+    os.makedirs(out_dir, exist_ok=True)
     for name, (n, d, k, lo, hi, sig, seed, budget, leaf, tol, h, mr, r) in CASES.items():
         X = S.gaussian_mixture(n, d, k, lo, hi, sig, None, seed)
         work = tempfile.mkdtemp(prefix="mxb_fixture_")

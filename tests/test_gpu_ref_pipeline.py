@@ -1,7 +1,7 @@
 """GPU: the drop-ins and the plan API on CDSs that the REFERENCE's own host pipeline produced.
 
 Two sources:
-* the committed fixtures ``tests/golden/ref_pipeline_*.npz``: the reference's structure
+* the committed fixtures ``tests/golden/ref_pipeline/*.npz``: the reference's structure
   generator, compression and ``DUV2CDS`` on seeded points, with the outputs of the evaluator
   the generator emitted for that structure (``Y_generated``) and of ``CBHGEMM`` /
   ``parHSSGEMM``;
@@ -25,7 +25,7 @@ from matrox_ru_b200 import _lib, hgemm as H, structure as S
 
 pytestmark = pytest.mark.gpu
 HERE = os.path.dirname(os.path.abspath(__file__))
-FIXTURES = sorted(glob.glob(os.path.join(HERE, "golden", "ref_pipeline_*.npz")))
+FIXTURES = sorted(glob.glob(os.path.join(HERE, "golden", "ref_pipeline", "*.npz")))
 FP64_TOL = 1e-12
 SPLIT_TOL = 1e-5
 

@@ -1,7 +1,7 @@
 """CPU: the reference's own host pipeline as the source of truth for the structure format,
 the structure builder and the oracle.
 
-The fixtures ``tests/golden/ref_pipeline_*.npz`` (``tests/golden/make_ref_pipeline.py``) hold
+The fixtures ``tests/golden/ref_pipeline/*.npz`` (``tests/golden/make_ref_pipeline.py``) hold
 what the REFERENCE's code produced for seeded points: the structure generator's ``.bin`` files
 (``sympiler/HTree.cpp:469-543``), the CDS exactly as ``DUV2CDS`` packs it
 (``matroxTest-V1/hcds.h:433-460``), and the outputs of the evaluator the generator emitted for
@@ -18,7 +18,7 @@ import ref_pipeline as RP
 from matrox_ru_b200 import structure as S, structure_bin as SB
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-FIXTURES = sorted(glob.glob(os.path.join(HERE, "golden", "ref_pipeline_*.npz")))
+FIXTURES = sorted(glob.glob(os.path.join(HERE, "golden", "ref_pipeline", "*.npz")))
 
 
 def load(path):
