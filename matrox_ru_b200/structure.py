@@ -25,9 +25,11 @@ Sympiler code generator.  It produces arrays in exactly the layout the reference
 * packing of near blocks ``D``, far couplings ``B`` and projections ``VT``
   (``matroxTest-V1/hcds.h:339-763``).
 
-Sampling of ID rows uses nearest outside points plus uniform random points instead of
-the reference's randomised-tree 32-NN search; the tree split fills a perfect tree
-(every level split) so the heap numbering the reference assumes always holds.
+ID rows are sampled as the reference samples them: k-NN sampling and pruning neighbours
+(``compression.h:362-443``) on 32-NN lists (the reference generator's own lists when a
+structure read from its files carries them, else exact lists laid out as the reference's
+max-heaps), then uniform random points.  The tree split fills a perfect tree (every level
+split) so the heap numbering the reference assumes always holds.
 """
 from __future__ import annotations
 
@@ -628,9 +630,154 @@ def _sample_rows(own: np.ndarray, cand: np.ndarray, nsamples: int, n: int,
     return np.concatenate(parts).astype(np.int64)
 
 
+# ---------------------------------------------------------------------------
+# k-NN sampling of ID rows (matroxTest-V1/compression.h:362-443, 597-797)
+# ---------------------------------------------------------------------------
+
+KNN = 32  # neighbours per point (sympiler/HTree.cpp:35, `setup.k = 32`)
+
+
+def _pair_gt(ad, ai, bd, bi):
+    """(distance, id) pairs compared lexicographically, as std::pair<double, int> compares."""
+    return (ad > bd) | ((ad == bd) & (ai > bi))
+
+
+def _max_heap_rows(d: np.ndarray, ids: np.ndarray) -> None:
+    """Arrange every row as a binary max-heap of (distance, id) pairs, in place.
+
+    The reference keeps each point's neighbour list as the max-heap of its search
+    (``sympiler/NearSearch.cpp:20-66`` leaves the lists unsorted), and its sampling reads the
+    first and second halves of that array (``compression.h:372-391``).  Exact lists built
+    here are given the same heap shape by a bottom-up heapify (Floyd's method)."""
+    n, k = d.shape
+    rows = np.arange(n)
+    for start in range(k // 2 - 1, -1, -1):
+        pos = np.full(n, start)
+        live = rows
+        while live.size:
+            p = pos[live]
+            c = 2 * p + 1
+            ok = c < k
+            live, p, c = live[ok], p[ok], c[ok]
+            if not live.size:
+                break
+            c2 = c + 1
+            has2 = c2 < k
+            c2s = np.where(has2, c2, c)
+            right = has2 & _pair_gt(d[live, c2s], ids[live, c2s], d[live, c], ids[live, c])
+            c = np.where(right, c2s, c)
+            swap = _pair_gt(d[live, c], ids[live, c], d[live, p], ids[live, p])
+            live, p, c = live[swap], p[swap], c[swap]
+            d[live, p], d[live, c] = d[live, c], d[live, p].copy()
+            ids[live, p], ids[live, c] = ids[live, c], ids[live, p].copy()
+            pos[live] = c
+
+
+def knn_lists(X: np.ndarray, k: int = KNN, chunk: int = 2048) -> Tuple[np.ndarray, np.ndarray]:
+    """Exact k nearest neighbours of every point (itself included) by squared Euclidean
+    distance: (ids, distances), each N x k, every row laid out as a max-heap like the
+    reference's lists.  Blocked distance products with torch (the GPU when one is present)."""
+    import torch
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    n = X.shape[0]
+    k = min(k, n)
+    dev = torch.device("cuda") if torch.cuda.is_available() else torch.device("cpu")
+    T = torch.as_tensor(X, device=dev)
+    sq = (T * T).sum(1)
+    ids = np.empty((n, k), np.int64)
+    dist = np.empty((n, k), np.float64)
+    for a in range(0, n, chunk):
+        b = min(n, a + chunk)
+        d2 = (sq[a:b, None] + sq[None, :] - 2.0 * (T[a:b] @ T.T)).clamp_min_(0.0)
+        d2[torch.arange(b - a, device=dev), torch.arange(a, b, device=dev)] = 0.0
+        val, idx = torch.topk(d2, k, dim=1, largest=False, sorted=True)
+        ids[a:b] = idx.cpu().numpy()
+        dist[a:b] = val.cpu().numpy()
+    # exact distances of the chosen pairs (the product form rounds), then ascending order
+    dist = ((X[ids] - X[:, None, :]) ** 2).sum(2)
+    order = np.lexsort((ids, dist), axis=1)
+    ids = np.take_along_axis(ids, order, 1)
+    dist = np.take_along_axis(dist, order, 1)
+    _max_heap_rows(dist, ids)
+    return ids, dist
+
+
+def _leaf_neighbours(NN, DN, own, nsamples):
+    """``BuildNeighBorsLeaf`` (compression.h:362-403): sampling neighbours of a leaf, in
+    (distance, id) order, and its pruning set.  The first half of each point's list is the
+    pruning set; the second half, sorted, gives the sampling neighbours outside both."""
+    k = NN.shape[1]
+    prune = np.setdiff1d(NN[own, :k // 2].ravel(), own)
+    tid = NN[own, (k + 1) // 2:].T.ravel()
+    tds = DN[own, (k + 1) // 2:].T.ravel()
+    order = np.lexsort((tid, tds))[: (k - 1) * len(own) // 2]
+    tid, tds = tid[order], tds[order]
+    keep = ~np.isin(tid, prune) & ~np.isin(tid, own)
+    tid, tds = tid[keep], tds[keep]
+    _, first = np.unique(tid, return_index=True)
+    first = np.sort(first)[:nsamples]
+    return tid[first], tds[first]
+
+
+def _internal_neighbours(lids, lds, rids, rds, own, lprune, rprune):
+    """``BuildNeighBorsInternal`` (compression.h:405-443): the children's sampling neighbours
+    merged (smallest distance per point), minus the node's points and the children's pruning
+    sets, in (distance, id) order."""
+    ids = np.concatenate([lids, rids])
+    ds = np.concatenate([lds, rds])
+    order = np.lexsort((ids, ds))
+    ids, ds = ids[order], ds[order]
+    _, first = np.unique(ids, return_index=True)
+    first = np.sort(first)
+    ids, ds = ids[first], ds[first]
+    keep = ~np.isin(ids, own) & ~np.isin(ids, lprune) & ~np.isin(ids, rprune)
+    return ids[keep], ds[keep]
+
+
+def _fill_random(amap: np.ndarray, own: np.ndarray, nsamples: int, n: int,
+                 rng: np.random.Generator) -> np.ndarray:
+    """The reference's sample rows (compression.h:622-650, 720-755): the neighbour rows
+    first, then uniform random points outside the node until ``nsamples``; every point when
+    ``nsamples`` reaches the number of outside points."""
+    if nsamples >= n - len(own):
+        return np.arange(n, dtype=np.int64)
+    taken = np.zeros(n, bool)
+    taken[own] = True
+    taken[amap] = True
+    parts = [np.asarray(amap, np.int64)]
+    need = nsamples - len(amap)
+    while need > 0:
+        draw = rng.integers(0, n, size=2 * need + 16)
+        draw = draw[~taken[draw]]
+        _, first = np.unique(draw, return_index=True)
+        draw = draw[np.sort(first)][:need]
+        taken[draw] = True
+        parts.append(draw)
+        need -= len(draw)
+    return np.concatenate(parts).astype(np.int64)
+
+
+def _fill_sequential(amap: np.ndarray, own: np.ndarray, nsamples: int, n: int, draw) -> np.ndarray:
+    """As :func:`_fill_random`, but one draw at a time from ``draw()`` (a source of the
+    values the reference's rand() returns), each accepted when it is neither a sample yet nor
+    a point of the node (compression.h:640-648)."""
+    if nsamples >= n - len(own):
+        return np.arange(n, dtype=np.int64)
+    out = [int(v) for v in amap]
+    taken = set(out)
+    taken.update(int(v) for v in own)
+    while len(out) < nsamples:
+        sample = draw() % n
+        if sample not in taken:
+            taken.add(sample)
+            out.append(sample)
+    return np.asarray(out, dtype=np.int64)
+
+
 def build_cds(X: np.ndarray, kernel: KernelSpec, leaf_size: int = 256, budget: float = 0.03,
               tol: float = 1e-5, max_rank: int = 256, seed: int = 0,
-              neighbour_leaves: int = 4, id_on_gpu: bool = False, structure=None) -> CDS:
+              neighbour_leaves: int = 4, id_on_gpu: bool = False, structure=None,
+              sampling: str = "knn", rand_source=None) -> CDS:
     """Build the CDS of the kernel matrix of point set X (N x d, row-major).
 
     ``id_on_gpu``: the sample matrices of each tree level are computed on the GPU
@@ -639,7 +786,21 @@ def build_cds(X: np.ndarray, kernel: KernelSpec, leaf_size: int = 256, budget: f
 
     ``structure``: a :class:`~matrox_ru_b200.structure_bin.Structure` (tree, near and far
     lists), e.g. read from the reference's ``.bin`` files, used instead of building one;
-    ``budget`` is then unused and ``leaf_size`` only sizes the samples."""
+    ``budget`` is then unused and ``leaf_size`` only sizes the samples.
+
+    ``sampling``: how the ID picks kernel rows outside a node.  "knn" (default) is the
+    reference's scheme (``compression.h:362-443, 597-797``) on 32-NN lists: the structure's
+    own lists when it carries them (the reference generator's ``NN.bin``), else exact lists
+    from :func:`knn_lists`.  "leaves" takes nearest outside points of the
+    ``neighbour_leaves`` closest leaves instead (no neighbour search).
+
+    ``rand_source``: a callable returning the successive values of the reference's rand()
+    (k-NN sampling only).  The random sample rows of every node are then drawn from it one
+    at a time, nodes in the reference's order (leaves, then each level upwards, node ids
+    ascending), so a single-threaded reference run is reproduced draw for draw; by default
+    each node draws from its own seeded generator."""
+    if sampling not in ("knn", "leaves"):
+        raise ValueError(f"sampling must be 'knn' or 'leaves', not {sampling!r}")
     X = np.ascontiguousarray(X, dtype=np.float64)
     n = X.shape[0]
     if structure is None:
@@ -664,7 +825,19 @@ def build_cds(X: np.ndarray, kernel: KernelSpec, leaf_size: int = 256, budget: f
 
     # neighbour candidates per leaf: outside points of the closest leaves, by distance
     cand: List[np.ndarray] = [np.zeros(0, np.int64)] * nn
-    if tree.nleaf > 1:
+    # k-NN sampling state per node: sampling neighbours (ids, distances) and pruning set
+    NN = DN = None
+    snb: List[Tuple[np.ndarray, np.ndarray]] = [(np.zeros(0, np.int64), np.zeros(0))] * nn
+    prune: List[np.ndarray] = [np.zeros(0, np.int64)] * nn
+    if sampling == "knn":
+        if structure is not None and structure.NN is not None and structure.distNN is not None \
+                and structure.NN.size == structure.distNN.size and structure.NN.size % n == 0:
+            k = structure.NN.size // n
+            NN = np.asarray(structure.NN, np.int64).reshape(n, k)
+            DN = np.asarray(structure.distNN, np.float64).reshape(n, k)
+        else:
+            NN, DN = knn_lists(X, KNN)
+    elif tree.nleaf > 1:
         dm = np.sqrt(sqdist(tree.mid, tree.mid))
         for i in range(tree.nleaf):
             order = [j for j in np.argsort(dm[i], kind="stable") if j != i][:neighbour_leaves]
@@ -677,7 +850,28 @@ def build_cds(X: np.ndarray, kernel: KernelSpec, leaf_size: int = 256, budget: f
     skels: List[np.ndarray] = [np.zeros(0, np.int64)] * nn
     proj: List[np.ndarray] = [np.zeros((0, 0))] * nn
 
+    def prepare_knn(v: int):
+        own = np.asarray(tree.lids[v], np.int64)
+        if lch[v] == -1:
+            bmap = own
+            nsamples = max(2 * len(bmap), 2 * leaf_size)
+            ids, ds = _leaf_neighbours(NN, DN, own, nsamples)
+            amap0 = ids
+        else:
+            l, r = int(lch[v]), int(rch[v])
+            bmap = np.concatenate([skels[l], skels[r]])
+            nsamples = max(2 * len(bmap), 2 * leaf_size)
+            ids, ds = _internal_neighbours(snb[l][0], snb[l][1], snb[r][0], snb[r][1], own, prune[l], prune[r])
+            amap0 = ids[:nsamples]
+        if rand_source is not None:
+            amap = _fill_sequential(amap0, own, nsamples, n, rand_source)
+        else:
+            amap = _fill_random(amap0, own, nsamples, n, np.random.default_rng([seed, v]))
+        return v, amap, bmap, (ids, ds)
+
     def prepare(v: int):
+        if NN is not None:
+            return prepare_knn(v)
         own = tree.lids[v]
         if lch[v] == -1:
             bmap = own
@@ -701,15 +895,22 @@ def build_cds(X: np.ndarray, kernel: KernelSpec, leaf_size: int = 256, budget: f
         amap = _sample_rows(own, cv, nsamples, n, np.random.default_rng([seed, v]))
         return v, amap, bmap, keep
 
-    def compress(v: int):
-        v, amap, bmap, keep = prepare(v)
+    def compress_prepared(prep):
+        v, amap, bmap, keep = prep
         K = kernel_matrix(X, amap, bmap, kernel)
         piv, P = interpolative_decomposition(np.asfortranarray(K), tol, max_rank)
         return v, bmap[piv], P, keep
 
+    def compress(v: int):
+        return compress_prepared(prepare(v))
+
+    def prepare_level(pool, nodes):
+        # one shared draw sequence: sample the level's nodes one after the other, in order
+        return [prepare(v) for v in nodes] if rand_source is not None else list(pool.map(prepare, nodes))
+
     def compress_level_on_gpu(pool, nodes):
         from . import hgemm as H
-        prep = list(pool.map(prepare, nodes))
+        prep = prepare_level(pool, nodes)
         K, _ = H.kernel_matrices(dX, kernel, [q[1] for q in prep], [q[2] for q in prep])
         ids = H.batched_id(K, [(len(q[1]), len(q[2])) for q in prep], tol, max_rank)
         del K
@@ -724,12 +925,22 @@ def build_cds(X: np.ndarray, kernel: KernelSpec, leaf_size: int = 256, budget: f
     with _blas_single_thread(), ThreadPoolExecutor(max_workers=_workers()) as pool:
         for lev in range(tree.depth, 0, -1):
             nodes = list(range((1 << lev) - 1, (1 << (lev + 1)) - 1))
-            level = compress_level_on_gpu(pool, nodes) if id_on_gpu else pool.map(compress, nodes)
+            if id_on_gpu:
+                level = compress_level_on_gpu(pool, nodes)
+            elif rand_source is not None and NN is not None:
+                level = pool.map(compress_prepared, prepare_level(pool, nodes))
+            else:
+                level = pool.map(compress, nodes)
             for v, sk, P, keep in level:
                 skels[v] = sk
                 proj[v] = P
                 slen[v] = P.shape[0]
-                if keep is not None:
+                if NN is not None:
+                    # the node's pruning set becomes its skeleton points' first half-lists
+                    # (compression.h:682-687, 783-788)
+                    snb[v] = keep
+                    prune[v] = np.unique(NN[np.asarray(sk, np.int64), :NN.shape[1] // 2].ravel())
+                elif keep is not None:
                     cand[v] = keep
 
     # ---- pack (hcds.h) ----

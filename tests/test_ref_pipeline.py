@@ -119,3 +119,54 @@ def test_reference_pipeline_reproduces_the_fixture(path, tmp_path):
                  workdir=str(tmp_path))
     for name, a in arrays.items():
         assert np.array_equal(run.arrays[name], a), name
+
+
+@pytest.mark.parametrize("path", FIXTURES, ids=os.path.basename)
+def test_producer_reproduces_the_reference_compression(path, tmp_path):
+    """structure.build_cds on the generator's files (its tree, lists and 32-NN lists), with
+    the reference's k-NN sampling and the reference's rand() sequence (one thread), makes the
+    reference's CDS: the same ranks, the same skeleton points in the same order, the same
+    blocks up to kernel rounding, and the same evaluation."""
+    from glibc_rand import GlibcRand
+    z, ref, arrays, files = load(path)
+    budget, leaf, tol, h, mr = z["params"]
+    write_files(files, str(tmp_path))
+    st = SB.read_structure(str(tmp_path), z["X"])
+    ours = S.build_cds(z["X"], S.KernelSpec("gaussian", h), leaf_size=int(leaf), budget=budget, tol=tol,
+                       max_rank=int(mr), structure=st, rand_source=GlibcRand())
+    assert np.array_equal(ours.slen, ref.slen)
+    for v in range(1, ref.numnodes):
+        assert np.array_equal(ours.skels[v], ref.skels[v]), v
+    for name in ("npairx", "npairy", "fpairx", "fpairy", "nblockset", "nblocks", "fblockset", "fblocks",
+                 "Ddim", "lchildren", "rchildren", "levelset", "idx", "cidx", "wpart", "clevelset"):
+        assert np.array_equal(getattr(ours, name), getattr(ref, name)), name
+    # blocks: the layouts of the pools may differ, compare block by block
+    for k in range(ref.ncount):
+        m = int(ref.Ddim[ref.npairx[k]]) * int(ref.Ddim[ref.npairy[k]])
+        a = ours.D[int(ours.Dptr[k]):int(ours.Dptr[k]) + m]
+        b = ref.D[int(ref.Dptr[k]):int(ref.Dptr[k]) + m]
+        assert np.abs(a - b).max() <= 1e-13
+    for k in range(ref.fcount):
+        m = int(ref.slen[ref.fpairx[k]]) * int(ref.slen[ref.fpairy[k]])
+        a = ours.B[int(ours.Bptr[k]):int(ours.Bptr[k]) + m]
+        b = ref.B[int(ref.Bptr[k]):int(ref.Bptr[k]) + m]
+        assert np.abs(a - b).max() <= 1e-13
+    scale = np.abs(ref.VT).max()
+    for v in range(1, ref.numnodes):
+        m = int(ref.slen[v]) * int(arrays["proj_column"][v])
+        a = ours.VT[int(ours.VTptr[v]):int(ours.VTptr[v]) + m]
+        b = ref.VT[int(ref.VTptr[v]):int(ref.VTptr[v]) + m]
+        assert np.abs(a - b).max() <= 1e-10 * scale, v
+    r = int(z["nrhs"][0])
+    got = O.eval_h2b(ours, z["TW"], r)
+    assert np.abs(got - z["Y_generated"]).max() <= 1e-11 * np.abs(z["Y_generated"]).max()
+
+
+def test_glibc_rand_restatement_matches_libc():
+    """The oracle's restatement of rand() (default seed) against the C library here."""
+    import ctypes
+    from glibc_rand import GlibcRand
+    libc = ctypes.CDLL("libc.so.6")
+    libc.srand(1)
+    g = GlibcRand()
+    assert all(g() == libc.rand() for _ in range(20000))
