@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--batched", action="store_true",
                     help="report instead of the benchmark: 64 uneven H2-b matrices in one merged, "
                          "graph-captured launch sequence vs the same plans evaluated one by one")
+    ap.add_argument("--c4", action="store_true",
+                    help="report instead of the benchmark: the differentiable kernel-ridge loss at N=262144, "
+                         "64 rhs (forward, adjoint and one loss + gradient step, FP64 traversals)")
     ap.add_argument("--tolerance-sweep", action="store_true",
                     help="accuracy report instead of the benchmark: the same points and kernel compressed "
                          "at ID tolerances 1e-3, 1e-5 and 1e-7, FP64 and split-BF16 (one JSON line each)")
@@ -162,6 +165,91 @@ def caller_order_timing(torch, H, plan, cds, TW, r, steps):
     out["layout"] = "W, Y row-major (N, r) in the caller's point order"
     del W, Y, Yu, TY
     return out
+
+
+def c4_report(args):
+    """Kernel-ridge loss L = 0.5 ||K~ W - Y||^2 on N=262144 points in d=18 (32-component mixture,
+    means uniform in [-2, 2]^18, sigma uniform in [0.3, 1.0]), Gaussian h=1.5, H2-b budget 0.03,
+    ID tolerance 1e-5, leaf 256, max rank 256; W and Y 262144 x 64 FP32 N(0, 1).  Device times
+    (CUDA events, inputs far larger than L2) of the forward K~ W and of the transposed traversal
+    K~^T G, in the leaf-blocked layout and in the caller's point order, and of one loss +
+    gradient step through the torch.autograd.Function; the gradient is checked against central
+    differences and the FP64 adjoint."""
+    import torch
+    from matrox_ru_b200 import build as mbuild, hgemm as H, structure as S
+    from matrox_ru_b200.autograd import KernelMatVec
+    mbuild.build()
+    dev = torch.device("cuda", 0)
+    t0 = time.time()
+    X = S.gaussian_mixture(262144, 18, 32, -2.0, 2.0, 0.3, 1.0, seed=4)
+    cds = S.build_cds(X, S.KernelSpec("gaussian", 1.5), leaf_size=256, budget=0.03, tol=1e-5, max_rank=256, seed=6)
+    t_build = time.time() - t0
+    r = 64
+    flops = cds.flops(r)
+    ev = H.Evaluator(cds)
+    cds_bytes = (cds.D.size + cds.B.size + cds.VT.size) * 8
+    g = torch.Generator(device=dev).manual_seed(7)
+    W = torch.randn(cds.n, r, device=dev, generator=g, dtype=torch.float32)
+    Yt = torch.randn(cds.n, r, device=dev, generator=g, dtype=torch.float32)
+    Wd, Yd = W.double(), Yt.double()
+    TW = ev.to_tree(Wd)
+    TG = ev.to_tree(Yd)
+    TY = torch.empty_like(TW)
+
+    def timed(fn, steps):
+        for _ in range(max(args.warmup, 3)):
+            fn()
+        torch.cuda.synchronize()
+        ev_ = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for a, b in ev_:
+            a.record()
+            fn()
+            b.record()
+        torch.cuda.synchronize()
+        return float(np.mean([a.elapsed_time(b) for a, b in ev_]))
+
+    fwd = timed(lambda: ev.plan.evaluate(TW, r, out=TY), args.steps)
+    adj = timed(lambda: ev.plan.adjoint(TG, r, out=TY), args.steps)
+    fwd_o = timed(lambda: ev(Wd), args.steps)
+    adj_o = timed(lambda: ev.adjoint(Yd), args.steps)
+
+    def step():
+        w = W.clone().requires_grad_()
+        loss = 0.5 * ((KernelMatVec.apply(w, ev) - Yt) ** 2).sum()
+        loss.backward()
+        return w.grad
+
+    step_ms = timed(step, args.steps)
+    grad32 = step()
+    # gradient checks: central differences along a random direction, and the FP64 adjoint
+    V = torch.randn(cds.n, r, device=dev, generator=g, dtype=torch.float64)
+    eps = 1e-2
+
+    def L(w):
+        return 0.5 * ((ev(w) - Yd) ** 2).sum().item()
+
+    fd = (L(Wd + eps * V) - L(Wd - eps * V)) / (2 * eps)
+    grad64 = ev.adjoint(ev(Wd) - Yd)
+    an = (grad64 * V).sum().item()
+    peak = fp64_peak_tflops(torch, dev)
+    line = {"report": "differentiable kernel-ridge loss (c4)", "n": cds.n, "d": 18, "nrhs": r,
+            "nleaf": cds.nleaf, "near_pairs": int(cds.ncount), "far_pairs": int(cds.fcount),
+            "cds_gb_fp64": round(cds_bytes / 1e9, 2), "flops_per_traversal": flops,
+            "forward_ms": round(fwd, 3), "adjoint_ms": round(adj, 3),
+            "forward_caller_order_ms": round(fwd_o, 3), "adjoint_caller_order_ms": round(adj_o, 3),
+            "loss_and_gradient_step_ms": round(step_ms, 3),
+            "forward_gflops": round(flops / (fwd * 1e-3) / 1e9, 1),
+            "adjoint_gflops": round(flops / (adj * 1e-3) / 1e9, 1),
+            "cds_stream_tb_per_s": {"forward": round(cds_bytes / (fwd * 1e-3) / 1e12, 2),
+                                    "adjoint": round(cds_bytes / (adj * 1e-3) / 1e12, 2)},
+            "fp64_peak_tflops_measured": round(peak, 2),
+            "frac_of_fp64_peak": {"forward": round(flops / (fwd * 1e-3) / 1e12 / peak, 3),
+                                  "adjoint": round(flops / (adj * 1e-3) / 1e12 / peak, 3)},
+            "grad_rel_err_fd": abs(fd - an) / abs(an),
+            "grad_fp32_vs_fp64_adjoint": float(torch.linalg.norm(grad32.double() - grad64) / torch.linalg.norm(grad64)),
+            "precision": "FP64 traversals (forward and adjoint); W, Y and the gradient FP32 at the torch boundary",
+            "cds_build_s": round(t_build, 1)}
+    print(json.dumps(line), flush=True)
 
 
 def tolerance_sweep(args, cfg):
@@ -381,6 +469,9 @@ def main():
         return
     if args.batched:
         batched_report(args)
+        return
+    if args.c4:
+        c4_report(args)
         return
     if args.impl == "reference":
         if world > 1:

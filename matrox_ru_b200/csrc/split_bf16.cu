@@ -1161,6 +1161,17 @@ int Batch::build(const std::vector<Plan *> &ps)
     return rc;
 }
 
+// Bytes of A tiles per group of coupling tasks in the unit order (0: longest task first, all
+// column tiles of a task together).  MXB_UNIT_GROUP_MB overrides the default.
+int64_t unit_group_bytes()
+{
+    static const int64_t v = [] {
+        const char *e = getenv("MXB_UNIT_GROUP_MB");
+        return (int64_t)((e && *e) ? atof(e) : 0.0) * (1 << 20);
+    }();
+    return v;
+}
+
 // Work units of every TC op for this entry's nrhs and column-tile choices.
 // The list is uploaded on `stream`, ahead of the launches that read it.
 int Batch::units_for(Entry &e, const std::vector<int> &bn, cudaStream_t stream)
@@ -1173,12 +1184,59 @@ int Batch::units_for(Entry &e, const std::vector<int> &bn, cudaStream_t stream)
         e.unit_first[k] = (int)units.size();
         if (m.phase == PH_SPLITW) continue;
         const bool pair = tile_pair(bn[k]);
-        for (int t = m.first; t < m.first + m.count; ++t) {
-            if (pair && tasks[t].m0 % 256) continue;  // the pair's odd CTA takes rows m0 + 128
-            const int ncol = (int)ceil_div(e.nrhs[tasks[t].plan], tile_width(bn[k]));
+        auto task_kt = [&](int t) {
             int kt = 0;
             for (int q = tasks[t].item0; q < tasks[t].item0 + tasks[t].nitem; ++q) kt += items[q].KT;
-            for (int c = 0; c < ncol; ++c) units.push_back(TcUnit{t, c, kt, 0});
+            return kt;
+        };
+        auto ncol_of = [&](int t) { return (int)ceil_div(e.nrhs[tasks[t].plan], tile_width(bn[k])); };
+        const int64_t group_bytes = unit_group_bytes();
+        if (group_bytes > 0 && (m.phase == PH_FARNEAR || m.phase == PH_FAR || m.phase == PH_NEAR)) {
+            // Coupling launches read each task's A tiles (CDS blocks) for every column tile and
+            // share the B tiles (W / skeleton slabs) among the tasks of neighbouring nodes.
+            // Tasks in tree order form groups whose A tiles fit in a slice of L2; a group
+            // sweeps its column tiles one after the other (all its tasks at column tile 0,
+            // then 1, ...), so its A tiles come from DRAM once and the in-flight units of one
+            // column tile share their B tiles.  Groups run heaviest first.
+            std::vector<int> ord;
+            for (int t = m.first; t < m.first + m.count; ++t)
+                if (!(pair && tasks[t].m0 % 256)) ord.push_back(t);
+            std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) {
+                const TcTask &x = tasks[a], &y = tasks[b];
+                if (x.plan != y.plan) return x.plan < y.plan;
+                if (x.out_kind != y.out_kind) return x.out_kind < y.out_kind;
+                if (x.c_row != y.c_row) return x.c_row < y.c_row;
+                return x.m0 < y.m0;
+            });
+            std::vector<std::pair<int64_t, std::vector<int>>> groups;  // (cost, tasks)
+            int64_t bytes = 0;
+            for (int t : ord) {
+                const int kt = task_kt(t);
+                const int64_t a = (int64_t)kt * m.P * TILE_BYTES * (pair ? 2 : 1);
+                if (groups.empty() || bytes + a > group_bytes) {
+                    groups.push_back({0, {}});
+                    bytes = 0;
+                }
+                groups.back().second.push_back(t);
+                groups.back().first += (int64_t)kt * ncol_of(t);
+                bytes += a;
+            }
+            std::stable_sort(groups.begin(), groups.end(),
+                             [](const auto &a, const auto &b) { return a.first > b.first; });
+            for (const auto &g : groups) {
+                int maxc = 0;
+                for (int t : g.second) maxc = std::max(maxc, ncol_of(t));
+                for (int c = 0; c < maxc; ++c)
+                    for (int t : g.second)
+                        if (c < ncol_of(t)) units.push_back(TcUnit{t, c, task_kt(t), 0});
+            }
+        } else {
+            for (int t = m.first; t < m.first + m.count; ++t) {
+                if (pair && tasks[t].m0 % 256) continue;  // the pair's odd CTA takes rows m0 + 128
+                const int ncol = ncol_of(t);
+                const int kt = task_kt(t);
+                for (int c = 0; c < ncol; ++c) units.push_back(TcUnit{t, c, kt, 0});
+            }
         }
         e.unit_count[k] = (int)units.size() - e.unit_first[k];
     }
@@ -1194,6 +1252,7 @@ int Batch::units_for(Entry &e, const std::vector<int> &bn, cudaStream_t stream)
 namespace {
 int kchain_for(int P);
 }
+
 
 int Batch::enqueue(Entry &e, cudaStream_t stream, int debug_flags, long long wait_cycles, const std::vector<int> &bn,
                    int only_op)
