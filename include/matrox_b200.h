@@ -263,6 +263,13 @@ MXB_API int32_t mxb_plan_status(mxb_plan *plan);
  * wait_cycles > 0 shortens every kernel wait limit (default ~4e9 SM cycles).  flags = 0
  * restores normal operation.  Split-BF16 plans only. */
 #define MXB_DEBUG_STALL_ONE_WAIT 1
+/* MXB_DEBUG_CHAIN_LEVELS: every run of consecutive up-sweep (or down-sweep) launches of one
+ * product count runs as one launch whose levels wait for each other on the device (otherwise
+ * the autotuner chains a run only where that is faster).  MXB_DEBUG_STALL_LEVEL (implies
+ * chaining): the first level of each chained launch never reports its units done, so the
+ * bounded wait of the next level runs out and mxb_plan_status() reports MXB_ERR_TIMEOUT. */
+#define MXB_DEBUG_CHAIN_LEVELS 2
+#define MXB_DEBUG_STALL_LEVEL 4
 MXB_API int32_t mxb_plan_set_test_hooks(mxb_plan *plan, int32_t flags, int64_t wait_cycles);
 /* Copies the last evaluation's skeleton workspaces (wskel, uskel) to host arrays laid out
  * with the caller's wskeloffset / uskeloffset (for callers that inspect them). */
@@ -317,6 +324,9 @@ typedef struct mxb_op_profile {
     double issued_flops;  /* tensor-pipe flops issued: padded tiles, x3 / x6 for split products */
     float ms;             /* device time of the launch */
     int32_t pair;         /* 1: runs on pairs of SMs (256-row tiles) */
+    int32_t chained;      /* 1: ran inside the launch of the record before it, as a later tree
+                             level that waits on the device for the level before; ms is 0 and
+                             that launch's ms covers both */
 } mxb_op_profile;
 /* `*nops` receives the number of launches; at most `cap` records are written. */
 MXB_API int32_t mxb_plan_profile(mxb_plan *plan, const double *dW, double *dY, int32_t nrhs, void *stream,

@@ -27,6 +27,8 @@ PREC_SPLIT_BF16_X6 = 3
 FLAG_MIRROR_WORKSPACES = 1
 FLAG_OUTPUT_IS_ZERO = 2
 DEBUG_STALL_ONE_WAIT = 1
+DEBUG_CHAIN_LEVELS = 2
+DEBUG_STALL_LEVEL = 4
 TILE_PAIR = 4096
 KERNEL_KINDS = {"gaussian": 0, "imq": 1, "newton": 2}
 PHASES = {0: "split_w", 1: "up", 2: "far", 3: "down", 4: "near", 5: "leaf_down", 6: "far_down",
@@ -61,7 +63,7 @@ class CdsDesc(ctypes.Structure):
 class OpProfile(ctypes.Structure):
     _fields_ = [("phase", I32), ("level", I32), ("width", I32), ("units", I32),
                 ("flops", ctypes.c_double), ("issued_flops", ctypes.c_double), ("ms", ctypes.c_float),
-                ("pair", I32)]
+                ("pair", I32), ("chained", I32)]
 
 
 _REF_ARGS_H2B = [P] * 12 + [I32] + [P] * 9 + [P] * 8  # up to fpairy

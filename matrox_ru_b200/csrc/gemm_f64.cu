@@ -36,6 +36,12 @@ __device__ __forceinline__ void cp_async8(double *dst, const double *src, bool v
     const int n = valid ? 8 : 0;  // 0 source bytes: the 8 destination bytes are zero-filled
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(src), "r"(n));
 }
+// 16 bytes (two doubles); `bytes` < 16 copies that many and zero-fills the rest
+__device__ __forceinline__ void cp_async16(double *dst, const double *src, int bytes)
+{
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(src), "r"(bytes));
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
@@ -53,6 +59,7 @@ struct Loader {
     int lda, ldb, K, trans;
     int k0;
     int q;
+    bool a16, b16;  // pairs of doubles along the contiguous dimension are 16-byte aligned
 };
 
 __device__ __forceinline__ const double *operand_ptr(const Operands &ops, int kind, int64_t row)
@@ -77,6 +84,10 @@ __device__ __forceinline__ void load_item(Loader &L, const Item *items, const Op
     L.K = it.K;
     L.trans = it.trans;
     L.k0 = 0;
+    // tile rows m0 and K offsets k0 are even, so every pair starts 16-byte aligned when the
+    // block does and its leading dimension is even
+    L.a16 = !it.trans && ((reinterpret_cast<uintptr_t>(L.A) & 15) == 0) && !(it.lda & 1);
+    L.b16 = ((reinterpret_cast<uintptr_t>(L.B) & 15) == 0) && !(it.ldb & 1);
 }
 
 __global__ void __launch_bounds__(THREADS, 4)
@@ -105,7 +116,17 @@ gemm_f64_kernel(const Task *__restrict__ tasks, const Item *__restrict__ items, 
         double *As = smem + stage * STAGE;
         double *Bs = As + A_TILE;
         const int k0 = L.k0;
-        if (!L.trans) {
+        if (L.a16) {
+            // two consecutive rows per copy: 16 bytes, the second zero-filled past M
+#pragma unroll
+            for (int i = 0; i < (BM * BK) / (2 * THREADS); ++i) {
+                const int idx = tid + i * THREADS;
+                const int m = (idx & (BM / 2 - 1)) * 2, k = idx / (BM / 2);
+                const int nv = (k0 + k < L.K) ? max(0, min(2, t.M - (t.m0 + m))) : 0;
+                const double *src = nv ? L.A + (size_t)(t.m0 + m) + (size_t)(k0 + k) * L.lda : L.A;
+                cp_async16(As + k * A_LD + m, src, nv * 8);
+            }
+        } else if (!L.trans) {
 #pragma unroll
             for (int i = 0; i < (BM * BK) / THREADS; ++i) {
                 const int idx = tid + i * THREADS;
@@ -124,13 +145,25 @@ gemm_f64_kernel(const Task *__restrict__ tasks, const Item *__restrict__ items, 
                 cp_async8(As + k * A_LD + m, src, v);
             }
         }
+        if (L.b16) {
+            // two consecutive K per copy
 #pragma unroll
-        for (int i = 0; i < (BN * BK) / THREADS; ++i) {
-            const int idx = tid + i * THREADS;
-            const int k = idx & (BK - 1), n = idx / BK;
-            const bool v = (k0 + k < L.K) && (n0 + n < nrhs);
-            const double *src = v ? L.B + (size_t)(k0 + k) + (size_t)(n0 + n) * L.ldb : L.B;
-            cp_async8(Bs + n * B_LD + k, src, v);
+            for (int i = 0; i < (BN * BK) / (2 * THREADS); ++i) {
+                const int idx = tid + i * THREADS;
+                const int k = (idx & (BK / 2 - 1)) * 2, n = idx / (BK / 2);
+                const int nv = (n0 + n < nrhs) ? max(0, min(2, L.K - (k0 + k))) : 0;
+                const double *src = nv ? L.B + (size_t)(k0 + k) + (size_t)(n0 + n) * L.ldb : L.B;
+                cp_async16(Bs + n * B_LD + k, src, nv * 8);
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < (BN * BK) / THREADS; ++i) {
+                const int idx = tid + i * THREADS;
+                const int k = idx & (BK - 1), n = idx / BK;
+                const bool v = (k0 + k < L.K) && (n0 + n < nrhs);
+                const double *src = v ? L.B + (size_t)(k0 + k) + (size_t)(n0 + n) * L.ldb : L.B;
+                cp_async8(Bs + n * B_LD + k, src, v);
+            }
         }
         L.k0 += BK;
     };

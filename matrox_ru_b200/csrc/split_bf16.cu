@@ -96,7 +96,7 @@ struct TcUnit {
     int32_t task;
     int32_t col;     // column tile: right-hand sides [col * BN, col * BN + BN)
     int32_t ktiles;  // K tiles of the task (sum over its items)
-    int32_t pad;
+    int32_t chain;   // chained launches: level << 20 | units of the level before (0: level 0)
 };
 
 struct SplitJob {     // one leaf block of W -> B-operand tiles
@@ -132,6 +132,13 @@ struct PlanArgs {
     int32_t pad;
 };
 
+// Tree levels one tensor-core launch may chain (consecutive ops of one product count and tile,
+// e.g. the up-sweep heights): the units of level j wait on the device until every unit of
+// level j - 1 has been written.
+constexpr int MAX_CHAIN = 24;
+// Tile-code flag (above MXB_TILE_PAIR): the op runs in the launch of the op before it.
+constexpr int TILE_CHAIN = 1 << 13;
+
 struct LaunchArgs {
     const PlanArgs *plans;
     const TcTask *tasks;
@@ -143,6 +150,9 @@ struct LaunchArgs {
     int nunits;
     int stall_test;         // test hook: CTA 0 withholds its first stage, so a wait runs out
     int kchain;             // K tiles accumulated per TMEM accumulator fill (1 or 2)
+    int nlevels;            // chained levels (1: none); a unit's level is in TcUnit::chain
+    int *level_done;        // per level: epilogue warps done with a unit of it (zero at launch)
+    int stall_level;        // test hook: level 0 never reports done, so level 1's waits run out
 };
 
 // ---------------------------------------------------------------------------------------
@@ -295,6 +305,7 @@ struct TcCfg {
     // and epilogue warps in a pair)
     static constexpr int RING_READERS = PAIR ? 2 * (1 + EPI_WARPS) + 1 : 1 + EPI_WARPS;
     static constexpr int THREADS = (EPI_WARPS + 2) * 32;
+    static constexpr int UNIT_WRITERS = EPI_WARPS * (PAIR ? 2 : 1);  // epilogue warps per unit
     static constexpr int COLS = BN / 2;          // accumulator columns per epilogue thread
     // old values loaded ahead of the stores in the epilogue's read-modify-writes (fewer where
     // 128 accumulators already fill the registers)
@@ -413,6 +424,7 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
             // ---------------- producer ----------------
             uint32_t g = 0;               // K-tile counter of this CTA
             uint32_t slot = 0;            // ring counter
+            int waited = 0;               // last chained level waited for
             uint32_t filled[C::STAGES];   // rounds filled per stage (drained before exit)
 #pragma unroll
             for (int s = 0; s < C::STAGES; ++s) filled[s] = 0;
@@ -448,6 +460,19 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                 }
                 if (u < 0) break;
                 const TcUnit un = la.units[u];
+                if (la.nlevels > 1) {
+                    // a unit of a chained level reads what the previous level wrote: wait until
+                    // every epilogue warp has finished every unit of that level
+                    const int lvl = un.chain >> 20;
+                    if (lvl > waited) {
+                        if (!tc::wait_counter(la.level_done + lvl - 1, (un.chain & 0xFFFFF) * C::UNIT_WRITERS,
+                                              abort_word, la.wait_cycles)) {
+                            raise_abort();
+                            break;
+                        }
+                        waited = lvl;
+                    }
+                }
                 const TcTask t = la.tasks[un.task];
                 const PlanArgs *pa = la.plans + t.plan;
                 const int NT = pa->NT;
@@ -823,6 +848,15 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                     }
                 }
             }
+            if (la.nlevels > 1) {
+                // this warp's part of the unit is stored: make it visible (also to the bulk
+                // copies of later levels) and count the warp done for the unit's level
+                asm volatile("fence.proxy.async.global;\n" ::: "memory");
+                __threadfence();
+                __syncwarp();
+                if (lane == 0 && !(la.stall_level && (un.chain >> 20) == 0))
+                    atomicAdd(la.level_done + (un.chain >> 20), 1);
+            }
         }
     }
     __syncwarp();
@@ -1023,6 +1057,7 @@ struct Batch : public mxb_batch {
     TcItem *dItems = nullptr;
     SplitJob *dJobs = nullptr;
     int *dNext = nullptr;  // work-unit counter per op
+    int *dLevel = nullptr; // per op: epilogue warps done with its units (chained launches)
     std::vector<void *> allocations;
     struct Entry {                     // one captured evaluation
         std::vector<const double *> W;
@@ -1068,6 +1103,7 @@ struct Batch : public mxb_batch {
     int enqueue(Entry &e, cudaStream_t stream, int debug_flags, long long wait_cycles, const std::vector<int> &bn,
                 int only_op = -1);
     int units_for(Entry &e, const std::vector<int> &bn, cudaStream_t stream);
+    void chain_all(std::vector<int> &bn) const;
     int tune(Entry &e, std::vector<PlanArgs> pa, std::vector<int> &bn, cudaStream_t stream, long long wait_cycles);
     Entry *find(const double *const *W, double *const *Y, const std::vector<int> &nr, int accumulate,
                 int debug_flags, const CallerOrder *order = nullptr);
@@ -1151,14 +1187,32 @@ int Batch::build(const std::vector<Plan *> &ps)
     if (!rc) rc = up((void **)&dItems, items.data(), items.size() * sizeof(TcItem));
     if (!rc) rc = up((void **)&dJobs, jobs.data(), jobs.size() * sizeof(SplitJob));
     if (!rc) {
-        cudaError_t e = cudaMalloc(&dNext, std::max<size_t>(ops.size(), 1) * sizeof(int));
+        cudaError_t e = cudaMalloc(&dNext, 2 * std::max<size_t>(ops.size(), 1) * sizeof(int));
         if (e != cudaSuccess) return batch_fail(std::string("batch allocation: ") + cudaGetErrorString(e), MXB_ERR_NOMEM);
         allocations.push_back(dNext);
+        dLevel = dNext + std::max<size_t>(ops.size(), 1);
     }
     // synchronous copies from pageable memory may return before their DMA lands, and the
     // evaluations run on streams that do not wait for the legacy stream
     if (!rc && cudaDeviceSynchronize() != cudaSuccess) rc = batch_fail("batch upload: synchronisation failed", MXB_ERR_CUDA);
     return rc;
+}
+
+// Runs of consecutive up-sweep ops, and of down-sweep ops with leaf down, that share a product
+// count and a tile; "family" 1 and 2, 0 for every other op.
+int chain_family(int phase) { return phase == PH_UP ? 1 : (phase == PH_DOWN || phase == PH_LEAFDOWN) ? 2 : 0; }
+
+void Batch::chain_all(std::vector<int> &bn) const
+{
+    for (size_t k = 0; k < ops.size();) {
+        const int fam = chain_family(ops[k].phase);
+        size_t j = k + 1;
+        while (fam && j < ops.size() && chain_family(ops[j].phase) == fam && ops[j].P == ops[k].P &&
+               (bn[j] & ~TILE_CHAIN) == (bn[k] & ~TILE_CHAIN) && j - k < (size_t)MAX_CHAIN)
+            ++j;
+        for (size_t q = k + 1; q < j; ++q) bn[q] |= TILE_CHAIN;
+        k = j;
+    }
 }
 
 // Bytes of A tiles per group of coupling tasks in the unit order (0: longest task first, all
@@ -1184,6 +1238,12 @@ int Batch::units_for(Entry &e, const std::vector<int> &bn, cudaStream_t stream)
         e.unit_first[k] = (int)units.size();
         if (m.phase == PH_SPLITW) continue;
         const bool pair = tile_pair(bn[k]);
+        // level of this op in its chained launch, and the units of the level before it
+        int level = 0;
+        for (size_t h = k; h > 0 && (bn[h] & TILE_CHAIN) && ops[h - 1].phase != PH_SPLITW; --h) ++level;
+        if (level >= MAX_CHAIN || (level && e.unit_count[k - 1] > 0xFFFFF))
+            return batch_fail("a chained launch exceeds its level or unit limits");
+        const int32_t chain = level ? (level << 20) | e.unit_count[k - 1] : 0;
         auto task_kt = [&](int t) {
             int kt = 0;
             for (int q = tasks[t].item0; q < tasks[t].item0 + tasks[t].nitem; ++q) kt += items[q].KT;
@@ -1228,14 +1288,14 @@ int Batch::units_for(Entry &e, const std::vector<int> &bn, cudaStream_t stream)
                 for (int t : g.second) maxc = std::max(maxc, ncol_of(t));
                 for (int c = 0; c < maxc; ++c)
                     for (int t : g.second)
-                        if (c < ncol_of(t)) units.push_back(TcUnit{t, c, task_kt(t), 0});
+                        if (c < ncol_of(t)) units.push_back(TcUnit{t, c, task_kt(t), chain});
             }
         } else {
             for (int t = m.first; t < m.first + m.count; ++t) {
                 if (pair && tasks[t].m0 % 256) continue;  // the pair's odd CTA takes rows m0 + 128
                 const int ncol = ncol_of(t);
                 const int kt = task_kt(t);
-                for (int c = 0; c < ncol; ++c) units.push_back(TcUnit{t, c, kt, 0});
+                for (int c = 0; c < ncol; ++c) units.push_back(TcUnit{t, c, kt, chain});
             }
         }
         e.unit_count[k] = (int)units.size() - e.unit_first[k];
@@ -1260,14 +1320,16 @@ int Batch::enqueue(Entry &e, cudaStream_t stream, int debug_flags, long long wai
     bool first_tc = true;
     int maxnt = 0;
     for (Plan *p : plans) maxnt = std::max(maxnt, p->bf16->nt_cap);
-    // work-unit counters of the tensor-core launches start at zero
-    cudaError_t zerr = only_op < 0 ? cudaMemsetAsync(dNext, 0, ops.size() * sizeof(int), stream)
-                                   : cudaMemsetAsync(dNext + only_op, 0, sizeof(int), stream);
+    // work-unit and level counters of the tensor-core launches start at zero (both arrays in
+    // one allocation: dLevel follows dNext)
+    const size_t nops = std::max<size_t>(ops.size(), 1);
+    cudaError_t zerr = cudaMemsetAsync(dNext, 0, 2 * nops * sizeof(int), stream);
     if (zerr != cudaSuccess) return batch_fail(std::string("work-unit counters: ") + cudaGetErrorString(zerr), MXB_ERR_CUDA);
     for (size_t k = 0; k < ops.size(); ++k) {
         const MOp &m = ops[k];
         const bool run = only_op < 0 || (int)k == only_op;
         cudaError_t err = cudaSuccess;
+        if (m.phase != PH_SPLITW && (bn[k] & TILE_CHAIN)) continue;  // runs in its chain head's launch
         if (m.phase == PH_SPLITW) {
             if (run) {
                 if (e.order.empty())
@@ -1289,7 +1351,19 @@ int Batch::enqueue(Entry &e, cudaStream_t stream, int debug_flags, long long wai
                 a.wait_cycles = wait_cycles > 0 ? wait_cycles : tc::WAIT_CYCLES;
                 a.stall_test = (debug_flags & MXB_DEBUG_STALL_ONE_WAIT) && first_tc;
                 a.kchain = kchain_for(m.P);
-                err = launch_tc(m.P, tile_width(bn[k]), tile_pair(bn[k]), m.writes_y && !e.order.empty(), a, stream);
+                // the ops chained to this one (same product count and tile) run as later levels
+                bool writes_y = m.writes_y;
+                size_t end = k + 1;
+                while (end < ops.size() && ops[end].phase != PH_SPLITW && (bn[end] & TILE_CHAIN))
+                    writes_y |= ops[end++].writes_y;
+                if (end - k > (size_t)MAX_CHAIN) return batch_fail("a chained launch has too many levels");
+                a.nlevels = (int)(end - k);
+                a.level_done = dLevel + k;
+                a.stall_level = (debug_flags & MXB_DEBUG_STALL_LEVEL) != 0;
+                int total = 0;
+                for (size_t j = k; j < end; ++j) total += e.unit_count[j];
+                a.nunits = total;
+                err = launch_tc(m.P, tile_width(bn[k]), tile_pair(bn[k]), writes_y && !e.order.empty(), a, stream);
             }
             first_tc = false;
         }
@@ -1368,13 +1442,19 @@ bool pairs_enabled()
     return on;
 }
 
+// MXB_TC_CHAIN=0 keeps every tree level in a launch of its own.
+// (read when an evaluation graph is built)
+bool chains_enabled()
+{
+    const char *e = getenv("MXB_TC_CHAIN");
+    return !(e && *e == '0');
+}
+
+// MXB_AUTOTUNE=0 keeps the default tiles (read when an evaluation graph is built).
 bool autotune_enabled()
 {
-    static const bool on = [] {
-        const char *e = getenv("MXB_AUTOTUNE");
-        return !(e && *e == '0');
-    }();
-    return on;
+    const char *e = getenv("MXB_AUTOTUNE");
+    return !(e && *e == '0');
 }
 
 }  // namespace
@@ -1411,6 +1491,7 @@ int Batch::tune(Entry &e, std::vector<PlanArgs> pa, std::vector<int> &bn, cudaSt
     te.dPlans = dTune;
     if (!rc && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
         rc = batch_fail("autotune events", MXB_ERR_CUDA);
+    std::vector<float> op_ms(ops.size(), 0.f);
     for (size_t k = 0; k < ops.size() && !rc; ++k) {
         if (ops[k].phase == PH_SPLITW) {
             rc = units_for(te, bn, stream);
@@ -1453,9 +1534,66 @@ int Batch::tune(Entry &e, std::vector<PlanArgs> pa, std::vector<int> &bn, cudaSt
             }
         }
         bn[k] = best_bn;
+        op_ms[k] = best;
         if (!rc) rc = units_for(te, bn, stream);
         if (!rc) rc = enqueue(te, stream, 0, wait_cycles, bn, (int)k);
     }
+    // Chains: a run of consecutive up-sweep launches (or down-sweep launches, leaf down
+    // included) of one product count may run as one launch whose levels wait for each other on
+    // the device.  Each run is timed chained, with every candidate tile shared by its levels,
+    // against the sum of its separately tuned launches; the faster is kept.  Every op's inputs
+    // are in place from the pass above, and re-running an op rewrites the same outputs.
+    for (size_t k = 0; k < ops.size() && !rc && chains_enabled();) {
+        const int fam = chain_family(ops[k].phase);
+        size_t j = k + 1;
+        while (fam && j < ops.size() && chain_family(ops[j].phase) == fam && ops[j].P == ops[k].P &&
+               j - k < (size_t)MAX_CHAIN)
+            ++j;
+        if (!fam || j - k < 2) {
+            k = j;
+            continue;
+        }
+        float separate = 0.f;
+        int max_m = 0;
+        for (size_t q = k; q < j; ++q) {
+            separate += op_ms[q];
+            max_m = std::max(max_m, ops[q].max_m);
+        }
+        std::vector<int> cands = ops[k].P == 2 ? std::vector<int>{256, 128, 64} : std::vector<int>{128, 64};
+        if (max_m > 128 && pairs_enabled()) cands.push_back(128 | MXB_TILE_PAIR);
+        float best = separate;
+        std::vector<int> best_bn;
+        for (int c : cands) {
+            if (tile_width(c) > 2 * std::max(64, maxn)) continue;
+            std::vector<int> trial = bn;
+            trial[k] = c;
+            for (size_t q = k + 1; q < j; ++q) trial[q] = c | TILE_CHAIN;
+            rc = units_for(te, trial, stream);
+            float ms = 0.f;
+            bool refused = false;
+            for (int rep = 0; rep < 2 && !rc && !refused; ++rep) {
+                cudaEventRecord(e0, stream);
+                const int lrc = enqueue(te, stream, 0, wait_cycles, trial, (int)k);
+                cudaEventRecord(e1, stream);
+                if (lrc) {
+                    refused = true;
+                    (void)cudaGetLastError();
+                    continue;
+                }
+                if (cudaEventSynchronize(e1) != cudaSuccess) rc = batch_fail("autotune sync", MXB_ERR_CUDA);
+                if (!rc) cudaEventElapsedTime(&ms, e0, e1);
+            }
+            if (rc) break;
+            if (refused) continue;
+            if (ms < best) {
+                best = ms;
+                best_bn = trial;
+            }
+        }
+        if (!best_bn.empty()) bn = best_bn;
+        k = j;
+    }
+    if (!rc) rc = units_for(te, bn, stream);
     if (!rc && cudaStreamSynchronize(stream) != cudaSuccess) rc = batch_fail("autotune sync", MXB_ERR_CUDA);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
@@ -1549,6 +1687,7 @@ int Batch::evaluate(const double *const *W, double *const *Y, const int *nrhs, i
             }
             tuned[nr] = bn;
         }
+        if (debug_flags & (MXB_DEBUG_CHAIN_LEVELS | MXB_DEBUG_STALL_LEVEL)) chain_all(bn);
         e.bn = bn;
         int rc = units_for(e, bn, stream);
         if (rc) {
@@ -1640,6 +1779,7 @@ int Batch::profile(const double *const *W, double *const *Y, const int *nrhs, cu
         o.level = m.level;
         o.width = tile_width(e->bn[k]);
         o.pair = tile_pair(e->bn[k]) ? 1 : 0;
+        o.chained = (m.phase != PH_SPLITW && (e->bn[k] & TILE_CHAIN)) ? 1 : 0;
         o.units = e->unit_count[k];
         const double products = m.P == 2 ? 3.0 : 6.0;
         const int tile_rows = o.pair ? 256 : 128;
@@ -1653,6 +1793,7 @@ int Batch::profile(const double *const *W, double *const *Y, const int *nrhs, cu
             }
         }
         cudaEventElapsedTime(&o.ms, ev[k], ev[k + 1]);
+        if (o.chained) o.ms = 0.f;
     }
     for (cudaEvent_t x : ev)
         if (x) cudaEventDestroy(x);
@@ -1926,7 +2067,21 @@ void Plan::clear_split_graphs()
 
 int split_bf16_prepare() { return configure_all_tc() == cudaSuccess ? MXB_OK : MXB_ERR_CUDA; }
 
-int split_bf16_launches(const Plan &p) { return p.bf16 ? (int)p.bf16->self->ops.size() : 0; }
+// Launches of an evaluation: one per op, less the ops chained into the launch before them in
+// the most recent evaluation graph.
+int launch_count(const Batch *b)
+{
+    if (!b) return 0;
+    int n = (int)b->ops.size();
+    if (!b->entries.empty()) {
+        const std::vector<int> &bn = b->entries.back().bn;
+        for (size_t k = 0; k < bn.size() && k < b->ops.size(); ++k)
+            if (b->ops[k].phase != PH_SPLITW && (bn[k] & TILE_CHAIN)) --n;
+    }
+    return n;
+}
+
+int split_bf16_launches(const Plan &p) { return p.bf16 ? launch_count(p.bf16->self) : 0; }
 
 Batch *split_bf16_batch(Plan &p) { return p.bf16 ? p.bf16->self : nullptr; }
 
@@ -2001,7 +2156,7 @@ int batch_status(Batch *b)
 
 void batch_destroy(Batch *b) { delete b; }
 
-int batch_launches(const Batch *b) { return b ? (int)b->ops.size() : 0; }
+int batch_launches(const Batch *b) { return launch_count(b); }
 
 int batch_tuned_widths(const Batch *b, int *widths, int cap)
 {

@@ -71,6 +71,26 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volati
     return true;
 }
 
+// Bounded wait until a global counter that other CTAs raise reaches `target` (acquire at GPU
+// scope), then a proxy fence so that the bulk copies this thread issues next (async proxy) see
+// the memory those CTAs wrote before raising it.  False when the wait gives up or an abort is
+// raised.
+__device__ __forceinline__ bool wait_counter(const int *ctr, int target, volatile int *abort_word,
+                                             long long limit = WAIT_CYCLES)
+{
+    const long long t0 = clock64();
+    for (;;) {
+        int v;
+        asm volatile("ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(ctr) : "memory");
+        if (v >= target) break;
+        if (*abort_word) return false;
+        if (clock64() - t0 > limit) return false;
+        __nanosleep(32);
+    }
+    asm volatile("fence.proxy.async.global;\n" ::: "memory");
+    return true;
+}
+
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
 {
     asm volatile(

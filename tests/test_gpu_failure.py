@@ -43,3 +43,57 @@ def test_hooks_rejected_on_fp64_plans(torch, small_cases):
     with pytest.raises(_lib.MxbError) as e:
         plan.set_test_hooks(_lib.DEBUG_STALL_ONE_WAIT)
     assert e.value.code == _lib.MXB_ERR_UNSUPPORTED
+
+
+def test_chained_levels_match_separate_launches(torch, small_cases):
+    """Up-sweep heights (and down-sweep depths with leaf down) run as one launch each, levels
+    waiting for each other on the device: the same result as the separate launches (the
+    evaluation is exact in the chaining; only the tile schedule changes), and fewer launches."""
+    import os
+    for name in ("h2b", "hss", "ragged"):
+        cds = small_cases[name]
+        r = 200
+        TW = torch.as_tensor(np.random.default_rng(3).standard_normal(cds.n * r), device="cuda")
+        # the default tiles, one launch per level
+        os.environ["MXB_TC_CHAIN"], os.environ["MXB_AUTOTUNE"] = "0", "0"
+        try:
+            sep = H.Plan(cds, "split_bf16")
+            want = sep.evaluate(TW, r).clone()
+            sep.status()
+        finally:
+            del os.environ["MXB_TC_CHAIN"], os.environ["MXB_AUTOTUNE"]
+        n_sep = sep.info()["launches"]
+        # the same tiles, levels chained: the same products in the same order, bit-identical
+        ch = H.Plan(cds, "split_bf16")
+        ch.set_test_hooks(_lib.DEBUG_CHAIN_LEVELS)
+        got = ch.evaluate(TW, r)
+        ch.status()
+        assert ch.info()["launches"] < n_sep, name
+        assert torch.equal(got, want), name
+        oracle = O.eval_h2b(cds, TW.cpu().numpy(), r)
+        err = np.linalg.norm(got.cpu().numpy() - oracle) / np.linalg.norm(oracle)
+        assert err <= 1e-5, (name, err)
+        prof = ch.profile(TW, r)
+        assert any(x["chained"] for x in prof)
+        assert all(x["ms"] == 0.0 for x in prof if x["chained"])
+
+
+def test_level_barrier_that_runs_out_reports_timeout(torch, small_cases):
+    """The first level of a chained launch never reports its units done (test hook): the
+    next level's bounded wait runs out, the plan reports MXB_ERR_TIMEOUT, and the same plan
+    then computes correctly."""
+    cds = small_cases["h2b"]
+    r = 64
+    TW = np.random.default_rng(4).standard_normal(cds.n * r)
+    want = O.eval_h2b(cds, TW, r)
+    plan = H.Plan(cds, "split_bf16")
+    tw = torch.as_tensor(TW, device="cuda")
+    plan.set_test_hooks(_lib.DEBUG_STALL_LEVEL, wait_cycles=100_000_000)  # ~50 ms limit
+    plan.evaluate(tw, r)
+    with pytest.raises(_lib.MxbError) as e:
+        plan.status()
+    assert e.value.code == _lib.MXB_ERR_TIMEOUT
+    plan.set_test_hooks(0)
+    got = plan.evaluate(tw, r).cpu().numpy()
+    plan.status()
+    assert np.linalg.norm(got - want) / np.linalg.norm(want) <= 1e-5
