@@ -279,12 +279,15 @@ MXB_API int32_t mxb_plan_read_workspaces(mxb_plan *plan, int32_t nrhs, const int
 /* ---- batches: many H-matrices in one launch sequence ---------------------------------------- */
 
 /* No counterpart in the reference (which evaluates one matrix per HGEMM call).  A batch merges
- * the launch sequences of several split-BF16 plans (same precision mode, same device; uneven
- * N, ranks and nrhs allowed): one tensor-core launch per level serves every plan, the whole
- * evaluation is captured as one CUDA graph, and the column-tile width of every launch is
- * picked by timing the candidates (64 / 128 / 256 right-hand sides) on the first evaluation of
- * an nrhs signature (MXB_AUTOTUNE=0 disables the measurement).  The plans must outlive the
- * batch; dW[i] / dY[i] are packed leaf-blocked device arrays of plan i with nrhs[i] columns. */
+ * the launch sequences of several split-BF16 plans (same device; uneven N, ranks and nrhs and
+ * any mix of split modes allowed -- couplings of different product counts run in separate
+ * launches): one tensor-core launch per level serves every plan, the whole evaluation is
+ * captured as one CUDA graph, and the column-tile width of every launch is picked by timing
+ * the candidates (64 / 128 / 256 right-hand sides) on the first evaluation of an nrhs
+ * signature (MXB_AUTOTUNE=0 disables the measurement); runs of up-sweep or down-sweep levels
+ * are chained into one launch with device-side level barriers where that measures faster.
+ * The plans must outlive the batch; dW[i] / dY[i] are packed leaf-blocked device arrays of
+ * plan i with nrhs[i] columns. */
 typedef struct mxb_batch mxb_batch;
 MXB_API int32_t mxb_batch_create(mxb_plan *const *plans, int32_t count, mxb_batch **out);
 MXB_API int32_t mxb_batch_evaluate(mxb_batch *batch, const double *const *dW, double *const *dY,

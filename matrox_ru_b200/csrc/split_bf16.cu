@@ -992,16 +992,19 @@ bool tile_pair(int code) { return (code & MXB_TILE_PAIR) != 0; }
 // count, the downward transfers by depth, the near field otherwise, then leaf down.  Phase
 // values are the MXB_PHASE_* codes of the profiling API.
 enum OpPhase { PH_SPLITW = 0, PH_UP = 1, PH_FAR = 2, PH_DOWN = 3, PH_NEAR = 4, PH_LEAFDOWN = 5, PH_FARNEAR = 8 };
-int64_t op_key(int phase, int level)
+// The product count is part of the key of the coupling ops, so plans of different split modes
+// (e.g. bf16x3 and bf16x6 far couplings) share a batch: their couplings run in separate
+// launches of the same stage of the sequence.
+int64_t op_key(int phase, int level, int P)
 {
     switch (phase) {
     case PH_SPLITW: return 0;
     case PH_UP: return 1 + level;
     case PH_FAR:
-    case PH_FARNEAR: return 100000;
-    case PH_DOWN: return 100000 + 1 + (int64_t)level;
-    case PH_NEAR: return 10000000;
-    default: return 10000001;
+    case PH_FARNEAR: return 1000000 + P;
+    case PH_DOWN: return 2000000 + (int64_t)level;
+    case PH_NEAR: return 3000000 + P;
+    default: return 4000000;
     }
 }
 
@@ -1115,11 +1118,10 @@ int Batch::build(const std::vector<Plan *> &ps)
 {
     if (ps.empty()) return batch_fail("empty batch");
     plans = ps;
-    const int prec = ps[0] ? ps[0]->precision : -1;
     MXB_CUDA_OR(cudaGetDevice(&device));
     for (Plan *p : ps) {
+        // any mix of split modes: the ops whose product counts differ run in separate launches
         if (!p || !p->bf16) return batch_fail("batches take split-BF16 plans");
-        if (p->precision != prec) return batch_fail("all plans of a batch must use the same precision mode");
         if (p->device != device) return batch_fail("all plans of a batch must live on the current device");
     }
     // merge ops by key, in key order; tasks and jobs get their plan index and offsets
@@ -1903,7 +1905,7 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
     }
     auto begin_op = [&](int phase, int level, int P) {
         Op o{};
-        o.key = op_key(phase, level);
+        o.key = op_key(phase, level, P);
         o.phase = phase;
         o.level = level;
         o.P = P;

@@ -108,3 +108,25 @@ def test_sixty_four_uneven_matrices_one_sequence(torch):
     batch.status()
     errs = [np.linalg.norm(o.cpu().numpy() - w) / np.linalg.norm(w) for o, w in zip(outs, wants)]
     assert max(errs) <= 1e-5, max(errs)
+
+
+def test_batch_mixes_split_modes(torch):
+    """Plans of different split modes share a batch (per-plan precision): couplings with 3
+    and 6 products run in separate launches; every result matches its plan evaluated alone."""
+    cases = make_cases(5, seed=7)
+    modes = ["split_bf16", "split_bf16_far6", "split_bf16", "split_bf16_x6", "split_bf16_far6"]
+    plans = [H.Plan(c, m) for (c, _), m in zip(cases, modes)]
+    batch = H.Batch(plans)
+    TWs, wants = [], []
+    for k, (c, r) in enumerate(cases):
+        TW = np.random.default_rng(30 + k).standard_normal(c.n * r)
+        TWs.append(torch.as_tensor(TW, device="cuda"))
+        wants.append(O.eval_h2b(c, TW, r))
+    nrhs = [r for _, r in cases]
+    outs = batch.evaluate(TWs, nrhs)
+    batch.status()
+    for (c, r), m, p, tw, o, want in zip(cases, modes, plans, TWs, outs, wants):
+        err = np.linalg.norm(o.cpu().numpy() - want) / np.linalg.norm(want)
+        assert 1e-12 < err <= (5e-6 if m != "split_bf16" else 1e-5), (m, err)
+        alone = p.evaluate(tw, r).cpu().numpy()
+        assert np.linalg.norm(alone - o.cpu().numpy()) <= 1e-6 * np.linalg.norm(want), m
