@@ -58,22 +58,40 @@ def test_batch_matches_oracle_and_single_plans(torch):
     assert np.linalg.norm(single.cpu().numpy() - outs[0].cpu().numpy()) <= 1e-6 * np.linalg.norm(wants[0])
 
 
+def pick_modes(torch, cases, TWs, kws, margin=8e-6):
+    """Per-plan precision, as the batch workload chooses it: the cheapest split mode whose
+    error against the FP64 oracle on the plan's own right-hand sides is within the margin."""
+    plans, modes = [], []
+    for (c, r), tw, kw in zip(cases, TWs, kws):
+        for mode in ("split_bf16", "split_bf16_far6", "split_bf16_x6"):
+            p = H.Plan(c, mode)
+            y = p.evaluate(tw, r).cpu().numpy()
+            p.status()
+            if np.linalg.norm(y - kw) / np.linalg.norm(kw) <= margin or mode == "split_bf16_x6":
+                break
+        plans.append(p)
+        modes.append(mode)
+    return plans, modes
+
+
 def test_batch_accumulates(torch):
     cases = make_cases(3, seed=5)
-    plans = [H.Plan(c, "split_bf16") for c, _ in cases]
-    batch = H.Batch(plans)
-    TWs, Y0s, wants = [], [], []
+    TWs, Y0s, kws = [], [], []
     for k, (c, r) in enumerate(cases):
         TW = np.random.default_rng(10 + k).standard_normal(c.n * r)
         Y0 = np.random.default_rng(20 + k).standard_normal(c.n * r)
         TWs.append(torch.as_tensor(TW, device="cuda"))
         Y0s.append(torch.as_tensor(Y0, device="cuda"))
-        wants.append(Y0 + O.eval_h2b(c, TW, r))  # accumulate = 1 adds, for HSS plans too
+        kws.append(O.eval_h2b(c, TW, r))
+    plans, modes = pick_modes(torch, cases, TWs, kws)
+    batch = H.Batch(plans)
     outs = [y.clone() for y in Y0s]
     batch.evaluate(TWs, [r for _, r in cases], outs=outs, accumulate=True)
     batch.status()
-    for o, want in zip(outs, wants):
-        assert np.linalg.norm(o.cpu().numpy() - want) / np.linalg.norm(want) <= 1e-5
+    for o, y0, kw, m in zip(outs, Y0s, kws, modes):
+        # accumulate = 1 adds, for HSS plans too
+        got = o.cpu().numpy() - y0.cpu().numpy()
+        assert np.linalg.norm(got - kw) / np.linalg.norm(kw) <= 1e-5, m
 
 
 def uneven_batch_cases(count, seed):

@@ -33,10 +33,12 @@ def test_profile_flops_and_result(torch, small_cases, name, precision):
     recs = plan.profile(TW, r, out=out)
     torch.cuda.synchronize()
     plan.status()
-    assert len(recs) == plan.info()["launches"]
+    # one record per op; ops chained into the launch before them (device-side level barriers)
+    # report ms 0, the launch's own record covers them
+    assert sum(not x["chained"] for x in recs) == plan.info()["launches"]
     assert sum(x["flops"] for x in recs) == plan.flops(r) == cds.flops(r)
     for x in recs:
-        assert x["ms"] > 0.0
+        assert (x["ms"] > 0.0) != x["chained"]
         assert x["issued_flops"] >= x["flops"]
         assert x["units"] > 0 or x["flops"] == 0  # units without items zero their output
     phases = {x["phase"] for x in recs}
@@ -64,7 +66,7 @@ def test_batch_profile(torch, small_cases):
     outs = [torch.zeros_like(w) for w in want]
     recs = batch.profile(TWs, [r for _, r in cases], outs)
     batch.status()
-    assert len(recs) == batch.info()["launches"]
+    assert sum(not x["chained"] for x in recs) == batch.info()["launches"]
     assert sum(x["flops"] for x in recs) == sum(c.flops(r) for c, r in cases)
     for o, w in zip(outs, want):
         torch.testing.assert_close(o, w, rtol=1e-13, atol=1e-13 * float(w.abs().max()))
