@@ -123,6 +123,15 @@ def batched_report(args, count=64, seed=20261204):
     batch_ms = timed(lambda: batch.evaluate(TWs, nrhs, outs=outs), args.steps)
     batch.status()
     errs = [float(torch.linalg.norm(o - y) / torch.linalg.norm(y)) for o, y in zip(outs, refs)]
+    # the same batch as ONE launch: W split and every level of every plan, device-side barriers
+    one = H.Batch(plans)
+    one.set_one_launch(True)
+    outs1 = [torch.zeros_like(t) for t in TWs]
+    one_ms = timed(lambda: one.evaluate(TWs, nrhs, outs=outs1), args.steps)
+    one.status()
+    errs1 = [float(torch.linalg.norm(o - y) / torch.linalg.norm(y)) for o, y in zip(outs1, refs)]
+    one_launches = one.info()["launches"]
+    del one, outs1
     single_ms = 0.0
     for p, t, r, o in zip(plans, TWs, nrhs, outs):
         single_ms += timed(lambda p=p, t=t, r=r, o=o: p.evaluate(t, r, out=o), args.steps)
@@ -130,6 +139,9 @@ def batched_report(args, count=64, seed=20261204):
     info = batch.info()
     line = {"report": "batched uneven H2-b matrices", "matrices": count, "algorithmic_flops": flops,
             "batch_ms": round(batch_ms, 3), "sum_of_single_plan_ms": round(single_ms, 3),
+            "one_launch": {"ms": round(one_ms, 3), "launches": one_launches,
+                           "tflops": round(flops / (one_ms * 1e-3) / 1e12, 2),
+                           "max_rel_err_vs_fp64_same_cds": max(errs1)},
             "batch_tflops": round(flops / (batch_ms * 1e-3) / 1e12, 2),
             "launches_per_batch_evaluation": info["launches"],
             "launches_single_plans": sum(p.info()["launches"] for p in plans),

@@ -270,6 +270,9 @@ MXB_API int32_t mxb_plan_status(mxb_plan *plan);
  * bounded wait of the next level runs out and mxb_plan_status() reports MXB_ERR_TIMEOUT. */
 #define MXB_DEBUG_CHAIN_LEVELS 2
 #define MXB_DEBUG_STALL_LEVEL 4
+/* MXB_DEBUG_ONE_LAUNCH: the plan's evaluation runs as one launch, as a batch in
+ * MXB_BATCH_ONE_LAUNCH mode does (with MXB_DEBUG_STALL_LEVEL, its level barriers run out). */
+#define MXB_DEBUG_ONE_LAUNCH 8
 MXB_API int32_t mxb_plan_set_test_hooks(mxb_plan *plan, int32_t flags, int64_t wait_cycles);
 /* Copies the last evaluation's skeleton workspaces (wskel, uskel) to host arrays laid out
  * with the caller's wskeloffset / uskeloffset (for callers that inspect them). */
@@ -300,6 +303,20 @@ MXB_API int32_t mxb_batch_status(mxb_batch *batch);
 #define MXB_TILE_PAIR 4096
 MXB_API int32_t mxb_batch_info(const mxb_batch *batch, int32_t *launches, int32_t *widths, int32_t cap,
                                int32_t *nwidths);
+/* How a batch evaluation is launched (no counterpart in the reference).
+ * MXB_BATCH_LEVEL_LAUNCHES (default): a W-split launch, then one tensor-core launch per level of
+ *   the merged sequence, runs of up-sweep or down-sweep levels chained into one launch where
+ *   the autotuner measures that faster.
+ * MXB_BATCH_ONE_LAUNCH: the whole evaluation -- the W split, up-sweep, couplings, near field,
+ *   down-sweep and leaf down of every plan -- is ONE launch of the persistent kernel: every
+ *   level is a group of work units that waits on the device (bounded) until the level before
+ *   it is written.  One column-tile width (64 or 128, timed on the first evaluation) and
+ *   3-part stages serve every level; units of bf16x3 couplings load 2 parts and issue 3
+ *   products.  W and Y leaf-blocked (MXB_ERR_UNSUPPORTED in the caller's point order).
+ * Changing the mode drops the batch's captured evaluations. */
+#define MXB_BATCH_LEVEL_LAUNCHES 0
+#define MXB_BATCH_ONE_LAUNCH 1
+MXB_API int32_t mxb_batch_set_launch_mode(mxb_batch *batch, int32_t mode);
 MXB_API int32_t mxb_batch_destroy(mxb_batch *batch);
 
 /* ---- per-launch timing (no counterpart in the reference, which times the whole HGEMM

@@ -29,6 +29,8 @@ FLAG_OUTPUT_IS_ZERO = 2
 DEBUG_STALL_ONE_WAIT = 1
 DEBUG_CHAIN_LEVELS = 2
 DEBUG_STALL_LEVEL = 4
+DEBUG_ONE_LAUNCH = 8
+BATCH_LEVEL_LAUNCHES, BATCH_ONE_LAUNCH = 0, 1
 TILE_PAIR = 4096
 KERNEL_KINDS = {"gaussian": 0, "imq": 1, "newton": 2}
 PHASES = {0: "split_w", 1: "up", 2: "far", 3: "down", 4: "near", 5: "leaf_down", 6: "far_down",
@@ -93,6 +95,7 @@ def load(path: str = LIB_PATH):
     lib.mxb_set_precision.argtypes = [I32]
     lib.mxb_set_flags.argtypes = [U32]
     lib.mxb_cache_set_mode.argtypes = [I32]
+    lib.mxb_batch_set_launch_mode.argtypes = [P, I32]
     lib.mxb_plan_create.argtypes = [ctypes.POINTER(CdsDesc), I32, ctypes.POINTER(P)]
     lib.mxb_plan_destroy.argtypes = [P]
     lib.mxb_plan_evaluate.argtypes = [P, P, P, I32, P, P, I32, P]

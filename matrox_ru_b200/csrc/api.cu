@@ -993,6 +993,15 @@ int32_t mxb_batch_info(const mxb_batch *batch, int32_t *launches, int32_t *width
     return MXB_OK;
 }
 
+int32_t mxb_batch_set_launch_mode(mxb_batch *batch, int32_t mode)
+{
+    if (!batch || (mode != MXB_BATCH_LEVEL_LAUNCHES && mode != MXB_BATCH_ONE_LAUNCH)) {
+        set_error("mxb_batch_set_launch_mode: null batch or unknown mode");
+        return MXB_ERR_ARG;
+    }
+    return batch_set_one_launch(reinterpret_cast<Batch *>(batch), mode == MXB_BATCH_ONE_LAUNCH);
+}
+
 int32_t mxb_batch_destroy(mxb_batch *batch)
 {
     batch_destroy(reinterpret_cast<Batch *>(batch));

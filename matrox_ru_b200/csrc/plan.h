@@ -107,6 +107,7 @@ int batch_evaluate(Batch *b, const double *const *W, double *const *Y, const int
 int batch_status(Batch *b);
 void batch_destroy(Batch *b);
 int batch_launches(const Batch *b);
+int batch_set_one_launch(Batch *b, int on);
 int batch_tuned_widths(const Batch *b, int *widths, int cap);
 int split_bf16_status(Plan &p);
 Batch *split_bf16_batch(Plan &p);  // the plan's own single-plan batch

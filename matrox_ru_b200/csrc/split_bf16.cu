@@ -76,6 +76,8 @@ enum OutKind : int16_t {
     OUT_Y = 0,      // FP64 Y block (leaf-blocked, caller's offsets)
     OUT_F32 = 1,    // FP32 skeleton block (a far result the down launch adds to)
     OUT_TILES = 2,  // skeleton block written as 3-part bf16 operand tiles for the next launches
+    OUT_SPLIT = 3,  // no product: one leaf's W block split into 3-part operand tiles (c_row:
+                    // leaf, out_kt: its K-tile base, M: its points; a unit's col: 128-column tile)
 };
 
 struct TcTask {
@@ -96,7 +98,8 @@ struct TcUnit {
     int32_t task;
     int32_t col;     // column tile: right-hand sides [col * BN, col * BN + BN)
     int32_t ktiles;  // K tiles of the task (sum over its items)
-    int32_t chain;   // chained launches: level << 20 | units of the level before (0: level 0)
+    int32_t chain;   // chained launches: parts << 28 | level << 20 | units of the level before
+                     // (parts 2 or 3: the unit's operand parts when they differ from the launch's)
 };
 
 struct SplitJob {     // one leaf block of W -> B-operand tiles
@@ -391,6 +394,11 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
         return u;
     };
 
+    // Operand parts of a unit (2: bf16x3 products, 3: bf16x6) and K tiles per accumulator fill:
+    // the launch's, or the unit's own in launches that mix both (those run with P = 3 stages).
+    auto unit_parts = [&](int32_t chain) { const int c = (chain >> 28) & 3; return c ? c : P; };
+    auto unit_kchain = [&](int parts) { return parts == P ? la.kchain : (parts == 2 ? 2 : 1); };
+
     if (threadIdx.x == 0) {
         for (int s = 0; s < C::STAGES; ++s) {
             tc::mbar_init(&full[s], 1);
@@ -463,7 +471,7 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                 if (la.nlevels > 1) {
                     // a unit of a chained level reads what the previous level wrote: wait until
                     // every epilogue warp has finished every unit of that level
-                    const int lvl = un.chain >> 20;
+                    const int lvl = (un.chain >> 20) & 0xFF;
                     if (lvl > waited) {
                         if (!tc::wait_counter(la.level_done + lvl - 1, (un.chain & 0xFFFFF) * C::UNIT_WRITERS,
                                               abort_word, la.wait_cycles)) {
@@ -482,7 +490,8 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                 // the odd CTA's rows may lie past the block: its A tile does not exist, and the
                 // MMA rows it feeds are never stored
                 const bool a_ok = !PAIR || issuer || t.m0 + 128 < t.M;
-                const uint32_t tx = (a_ok ? C::A_BYTES : 0) + C::B_BYTES;
+                const int up = unit_parts(un.chain);
+                const uint32_t tx = (a_ok ? (uint32_t)up * TILE_BYTES : 0u) + (uint32_t)up * C::B_ROWS_BYTES;
                 for (int q = 0; q < t.nitem && !stop; ++q) {
                     const TcItem it = ti[q];
                     const uint8_t *a_pool = pa->pool[it.a_pool];
@@ -500,8 +509,8 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                         uint8_t *sb = sa + C::A_BYTES;
                         tc::mbar_expect_tx(&full[s], tx);
                         if (a_ok) {
-                            const uint8_t *ga = a_pool + it.a_off + ((size_t)mt * it.KT + kt) * (size_t)P * TILE_BYTES;
-                            tc::bulk_g2s(sa, ga, C::A_BYTES, &full[s]);
+                            const uint8_t *ga = a_pool + it.a_off + ((size_t)mt * it.KT + kt) * (size_t)up * TILE_BYTES;
+                            tc::bulk_g2s(sa, ga, (uint32_t)up * TILE_BYTES, &full[s]);
                         }
                         if (C::B_ROWS >= 128) {
 #pragma unroll
@@ -511,8 +520,9 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                                     b_pool + ((size_t)it.b_base * NT + nt * it.KT + kt) * 3 * (size_t)TILE_BYTES;
 #pragma unroll
                                 for (int p = 0; p < P; ++p)
-                                    tc::bulk_g2s(sb + p * C::B_ROWS_BYTES + hh * TILE_BYTES, gb + (size_t)p * TILE_BYTES,
-                                                 TILE_BYTES, &full[s]);
+                                    if (p < up)
+                                        tc::bulk_g2s(sb + p * C::B_ROWS_BYTES + hh * TILE_BYTES,
+                                                     gb + (size_t)p * TILE_BYTES, TILE_BYTES, &full[s]);
                             }
                         } else {
                             // B_ROWS rows starting at row cb % 128 of a 128-row tile: contiguous, and
@@ -523,8 +533,9 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                                                 (size_t)(cb & 127) * 128;
 #pragma unroll
                             for (int p = 0; p < P; ++p)
-                                tc::bulk_g2s(sb + p * C::B_ROWS_BYTES, gb + (size_t)p * TILE_BYTES, C::B_ROWS_BYTES,
-                                             &full[s]);
+                                if (p < up)
+                                    tc::bulk_g2s(sb + p * C::B_ROWS_BYTES, gb + (size_t)p * TILE_BYTES, C::B_ROWS_BYTES,
+                                                 &full[s]);
                         }
                         filled[s] = round + 1;
                     }
@@ -555,13 +566,16 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                     if (u == -2) raise_abort();
                     break;
                 }
+                const int up = ktiles ? unit_parts(la.units[u].chain) : P;
+                const int nprod = up == 2 ? 3 : 6;
+                const int kc = unit_kchain(up);
                 for (int i = 0; i < ktiles; ++i, ++g) {
                     const int s = g % C::STAGES;
                     const uint32_t round = g / C::STAGES;
                     const int b = ga % C::NACC;
                     const uint32_t use = ga / C::NACC;
-                    const bool first = i % la.kchain == 0;
-                    const bool last = i % la.kchain == la.kchain - 1 || i == ktiles - 1;
+                    const bool first = i % kc == 0;
+                    const bool last = i % kc == kc - 1 || i == ktiles - 1;
                     if ((first && !wait_x(&acce[b], (use & 1) ^ 1, abort_word)) ||
                         !tc::mbar_wait(&full[s], round & 1, abort_word, la.wait_cycles) ||
                         (PAIR && !wait_x(&pfull[s], round & 1, abort_word))) {
@@ -580,6 +594,7 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                     for (int ks = 0; ks < 4; ++ks) {
 #pragma unroll
                         for (int j = 0; j < C::NPROD; ++j) {
+                            if (j >= nprod) break;
                             const uint64_t ad = da + (uint64_t)((PA[j] * TILE_BYTES + ks * 32) >> 4);
                             const uint64_t bd = db + (uint64_t)((PB[j] * C::B_ROWS_BYTES + ks * 32) >> 4);
                             if constexpr (PAIR) tc::mma_bf16_pair(dst, ad, bd, IDESC, accum);
@@ -645,7 +660,25 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
             }
             const TcUnit un = la.units[u];
             const TcTask t = la.tasks[un.task];
-            const int fills = (ktiles + la.kchain - 1) / la.kchain;
+            const int kc = unit_kchain(unit_parts(un.chain));
+            const int fills = (ktiles + kc - 1) / kc;
+            if (la.nlevels > 1 && ((un.chain >> 20) & 0xFF) > 0) {
+                // the old values this unit reads back (Y, the far result) may come from an
+                // earlier level of this launch: acquire that level's completion here too (the
+                // producer's wait covers only its bulk copies).  Lane 0 waits; then every lane
+                // takes its own acquire of the completed count.
+                const int lvl = (un.chain >> 20) & 0xFF;
+                const int *ctr = la.level_done + lvl - 1;
+                int done = 1;
+                if (lane == 0)
+                    done = tc::wait_counter(ctr, (un.chain & 0xFFFFF) * C::UNIT_WRITERS, abort_word, la.wait_cycles);
+                done = __shfl_sync(0xffffffffu, done, 0);
+                if (!done) {
+                    if (lane == 0) raise_abort();
+                    break;
+                }
+                tc::acquire_counter(ctr);
+            }
             {
                 // The output phase reads old values (Y, the far result) with a few loads in
                 // flight per thread: ask L2 for them now, so the unit's MMAs cover the DRAM
@@ -804,6 +837,29 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                         if (cc < nrhs) Sb[(size_t)cc * t.ldc] = acc[e];
                     }
                 }
+            } else if (t.out_kind == OUT_SPLIT) {
+                // no product: split one 128-column tile of a leaf's W block (FP64, leaf-blocked)
+                // into 3-part operand tiles, every K tile of the leaf, as split_w_kernel does.
+                // Columns past nrhs and points past M are zero.
+                const int nt = un.col;
+                const int KTv = (t.M + 63) / 64;
+                const double *src = pa->W + pa->wofs[t.c_row];
+                uint8_t *base = pa->buf[t.t_buf] + ((size_t)t.out_kt * pa->NT + (size_t)nt * KTv) * 3 * (size_t)TILE_BYTES;
+                const int tid = threadIdx.x;  // the epilogue warps are warps 0 .. EPI_WARPS - 1
+                for (int kt = 0; kt < KTv; ++kt) {
+                    for (int idx = tid; idx < 1024; idx += C::EPI_WARPS * 32) {
+                        const int c = idx % 8, rr = idx / 8;
+                        const int n = nt * 128 + rr;
+                        __nv_bfloat16 h[8], m[8], l[8];
+#pragma unroll
+                        for (int e = 0; e < 8; ++e) {
+                            const int k = kt * 64 + c * 8 + e;
+                            const double x = (n < nrhs && k < t.M) ? src[k + (size_t)n * t.ldc] : 0.0;
+                            tc::split3(x, h[e], m[e], l[e]);
+                        }
+                        store_parts(base + (size_t)kt * 3 * TILE_BYTES, 3, rr, c, h, m, l);
+                    }
+                }
             } else {
                 // OUT_TILES: (optionally) add the FP32 far result, then write this row's values
                 // as 3-part bf16 operand tiles.  The lane holds one K index; a transpose in
@@ -854,8 +910,8 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                 asm volatile("fence.proxy.async.global;\n" ::: "memory");
                 __threadfence();
                 __syncwarp();
-                if (lane == 0 && !(la.stall_level && (un.chain >> 20) == 0))
-                    atomicAdd(la.level_done + (un.chain >> 20), 1);
+                const int lvl = (un.chain >> 20) & 0xFF;
+                if (lane == 0 && !(la.stall_level && lvl == 0)) atomicAdd(la.level_done + lvl, 1);
             }
         }
     }
@@ -1055,6 +1111,10 @@ struct Batch : public mxb_batch {
     std::vector<MOp> ops;
     std::vector<TcTask> tasks;
     std::vector<TcItem> items;
+    // One-launch mode: the W split and every tensor-core op run as the levels of a single
+    // launch of the kernel with 3-part stages (OUT_SPLIT tasks at [split_task0, + split_tasks)).
+    bool one_launch = false;
+    int split_task0 = 0, split_tasks = 0;
     std::vector<SplitJob> jobs;
     TcTask *dTasks = nullptr;
     TcItem *dItems = nullptr;
@@ -1108,6 +1168,8 @@ struct Batch : public mxb_batch {
     int units_for(Entry &e, const std::vector<int> &bn, cudaStream_t stream);
     void chain_all(std::vector<int> &bn) const;
     int tune(Entry &e, std::vector<PlanArgs> pa, std::vector<int> &bn, cudaStream_t stream, long long wait_cycles);
+    int tune_one_launch(Entry &e, std::vector<PlanArgs> pa, std::vector<int> &bn, cudaStream_t stream,
+                        long long wait_cycles);
     Entry *find(const double *const *W, double *const *Y, const std::vector<int> &nr, int accumulate,
                 int debug_flags, const CallerOrder *order = nullptr);
     int profile(const double *const *W, double *const *Y, const int *nrhs, cudaStream_t stream, mxb_op_profile *out,
@@ -1177,6 +1239,24 @@ int Batch::build(const std::vector<Plan *> &ps)
         }
         if (m.count > 0) ops.push_back(m);
     }
+    // the W split as tasks of the tensor-core kernel, for the one-launch mode
+    split_task0 = (int)tasks.size();
+    for (const MOp &m : ops) {
+        if (m.phase != PH_SPLITW) continue;
+        for (int j = m.first; j < m.first + m.count; ++j) {
+            const SplitJob &sj = jobs[j];
+            TcTask t{};
+            t.c_row = sj.src_row;
+            t.out_kt = sj.dst_kt;
+            t.ldc = sj.ld;
+            t.M = sj.K;
+            t.plan = sj.plan;
+            t.out_kind = OUT_SPLIT;
+            t.t_buf = BUF_W;
+            tasks.push_back(t);
+        }
+    }
+    split_tasks = (int)tasks.size() - split_task0;
     auto up = [&](void **dst, const void *src, size_t bytes) -> int {
         cudaError_t e = cudaMalloc(dst, std::max<size_t>(bytes, 16));
         if (e != cudaSuccess) return batch_fail(std::string("batch allocation: ") + cudaGetErrorString(e), MXB_ERR_NOMEM);
@@ -1235,7 +1315,34 @@ int Batch::units_for(Entry &e, const std::vector<int> &bn, cudaStream_t stream)
     std::vector<TcUnit> units;
     e.unit_first.assign(ops.size(), 0);
     e.unit_count.assign(ops.size(), 0);
-    for (size_t k = 0; k < ops.size(); ++k) {
+    if (one_launch) {
+        // level k = op k: the W split (one unit per leaf and 128-column tile), then every
+        // tensor-core op in sequence, each unit tagged with its operand parts
+        if (ops.size() > (size_t)MAX_CHAIN) return batch_fail("too many levels for one launch");
+        for (size_t k = 0; k < ops.size(); ++k) {
+            const MOp &m = ops[k];
+            e.unit_first[k] = (int)units.size();
+            const int prev = k ? e.unit_count[k - 1] : 0;
+            if (prev > 0xFFFFF) return batch_fail("a level of the one-launch evaluation has too many units");
+            const int32_t chain = ((int32_t)k << 20) | prev;
+            if (m.phase == PH_SPLITW) {
+                for (int t = split_task0; t < split_task0 + split_tasks; ++t) {
+                    const int NT = plans[tasks[t].plan]->bf16->nt_cap;
+                    for (int nt = 0; nt < NT; ++nt) units.push_back(TcUnit{t, nt, 0, chain | (3 << 28)});
+                }
+            } else {
+                const int w = tile_width(bn[k]);
+                for (int t = m.first; t < m.first + m.count; ++t) {
+                    int kt = 0;
+                    for (int q = tasks[t].item0; q < tasks[t].item0 + tasks[t].nitem; ++q) kt += items[q].KT;
+                    const int ncol = (int)ceil_div(e.nrhs[tasks[t].plan], w);
+                    for (int c = 0; c < ncol; ++c) units.push_back(TcUnit{t, c, kt, chain | (m.P << 28)});
+                }
+            }
+            e.unit_count[k] = (int)units.size() - e.unit_first[k];
+        }
+    }
+    for (size_t k = 0; k < ops.size() && !one_launch; ++k) {
         const MOp &m = ops[k];
         e.unit_first[k] = (int)units.size();
         if (m.phase == PH_SPLITW) continue;
@@ -1327,6 +1434,34 @@ int Batch::enqueue(Entry &e, cudaStream_t stream, int debug_flags, long long wai
     const size_t nops = std::max<size_t>(ops.size(), 1);
     cudaError_t zerr = cudaMemsetAsync(dNext, 0, 2 * nops * sizeof(int), stream);
     if (zerr != cudaSuccess) return batch_fail(std::string("work-unit counters: ") + cudaGetErrorString(zerr), MXB_ERR_CUDA);
+    if (one_launch) {
+        // every op is a level of the launch of op 0 (profiling asks for op 0 to time it)
+        if (only_op > 0) return MXB_OK;
+        int w = 128;
+        for (size_t k = 0; k < ops.size(); ++k)
+            if (ops[k].phase != PH_SPLITW) {
+                w = tile_width(bn[k]) >= 128 ? 128 : 64;
+                break;
+            }
+        LaunchArgs a{};
+        a.plans = e.dPlans;
+        a.tasks = dTasks;
+        a.items = dItems;
+        a.units = e.dUnits;
+        a.nunits = 0;
+        for (int c : e.unit_count) a.nunits += c;
+        a.next_unit = dNext;
+        a.err = plans[0]->bf16->dErr;
+        a.wait_cycles = wait_cycles > 0 ? wait_cycles : tc::WAIT_CYCLES;
+        a.stall_test = (debug_flags & MXB_DEBUG_STALL_ONE_WAIT) != 0;
+        a.kchain = kchain_for(3);
+        a.nlevels = (int)ops.size();
+        a.level_done = dLevel;
+        a.stall_level = (debug_flags & MXB_DEBUG_STALL_LEVEL) != 0;
+        const cudaError_t err = launch_tc(3, w, false, false, a, stream);
+        if (err != cudaSuccess) return batch_fail(std::string("one-launch evaluation: ") + cudaGetErrorString(err), MXB_ERR_CUDA);
+        return MXB_OK;
+    }
     for (size_t k = 0; k < ops.size(); ++k) {
         const MOp &m = ops[k];
         const bool run = only_op < 0 || (int)k == only_op;
@@ -1464,8 +1599,72 @@ bool autotune_enabled()
 // Autotuner: runs the op sequence once; every tensor-core op is timed with each candidate
 // column-tile width (second of two runs, CUDA events) with the Y outputs redirected to
 // scratch, and the fastest width is kept.  Each op's outputs are left in place for the next.
+// One-launch mode: the whole evaluation is one launch, so its one column-tile width (64 or 128)
+// is picked by timing the launch with each (Y redirected to scratch).
+int Batch::tune_one_launch(Entry &e, std::vector<PlanArgs> pa, std::vector<int> &bn, cudaStream_t stream,
+                           long long wait_cycles)
+{
+    const int np = (int)plans.size();
+    std::vector<double *> scratch(np, nullptr);
+    PlanArgs *dTune = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    Entry te;
+    te.nrhs = e.nrhs;
+    int rc = MXB_OK;
+    for (int i = 0; i < np && !rc; ++i) {
+        Plan &p = *plans[i];
+        size_t ext = 0;
+        for (int l = 0; l < p.nleaf; ++l)
+            ext = std::max<size_t>(ext, (size_t)p.ofs_host[1][l] + (size_t)p.Ddim[l] * e.nrhs[i]);
+        if (cudaMalloc(&scratch[i], std::max<size_t>(ext, 1) * sizeof(double)) != cudaSuccess)
+            rc = batch_fail("autotune scratch allocation failed", MXB_ERR_NOMEM);
+        else
+            pa[i].Y = scratch[i];
+        pa[i].y_perm = nullptr;
+    }
+    if (!rc && cudaMalloc(&dTune, np * sizeof(PlanArgs)) != cudaSuccess)
+        rc = batch_fail("autotune table allocation failed", MXB_ERR_NOMEM);
+    if (!rc && cudaMemcpyAsync(dTune, pa.data(), np * sizeof(PlanArgs), cudaMemcpyHostToDevice, stream) != cudaSuccess)
+        rc = batch_fail("autotune table upload failed", MXB_ERR_CUDA);
+    te.dPlans = dTune;
+    if (!rc && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
+        rc = batch_fail("autotune events", MXB_ERR_CUDA);
+    float best = 1e30f;
+    int best_w = 128;
+    for (int w : {128, 64}) {
+        if (rc) break;
+        std::vector<int> trial = bn;
+        for (size_t k = 0; k < ops.size(); ++k)
+            if (ops[k].phase != PH_SPLITW) trial[k] = w;
+        rc = units_for(te, trial, stream);
+        float ms = 0.f;
+        for (int rep = 0; rep < 2 && !rc; ++rep) {
+            cudaEventRecord(e0, stream);
+            rc = enqueue(te, stream, 0, wait_cycles, trial, -1);
+            cudaEventRecord(e1, stream);
+            if (!rc && cudaEventSynchronize(e1) != cudaSuccess) rc = batch_fail("autotune sync", MXB_ERR_CUDA);
+            if (!rc) cudaEventElapsedTime(&ms, e0, e1);
+        }
+        if (!rc && ms < best) {
+            best = ms;
+            best_w = w;
+        }
+    }
+    for (size_t k = 0; k < ops.size(); ++k)
+        if (ops[k].phase != PH_SPLITW) bn[k] = best_w;
+    if (!rc && cudaStreamSynchronize(stream) != cudaSuccess) rc = batch_fail("autotune sync", MXB_ERR_CUDA);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (te.dUnits) cudaFree(te.dUnits);
+    if (dTune) cudaFree(dTune);
+    for (double *x : scratch)
+        if (x) cudaFree(x);
+    return rc;
+}
+
 int Batch::tune(Entry &e, std::vector<PlanArgs> pa, std::vector<int> &bn, cudaStream_t stream, long long wait_cycles)
 {
+    if (one_launch) return tune_one_launch(e, pa, bn, stream, wait_cycles);
     const int np = (int)plans.size();
     const int maxn = *std::max_element(e.nrhs.begin(), e.nrhs.end());
     std::vector<double *> scratch(np, nullptr);
@@ -1614,6 +1813,7 @@ int Batch::evaluate(const double *const *W, double *const *Y, const int *nrhs, i
     MXB_CUDA_OR(cudaGetDevice(&cur));
     if (cur != device) return batch_fail("batch used on a different device than it was created on");
     std::vector<int> nr(nrhs, nrhs + np);
+    if (one_launch && order) return batch_fail("the one-launch mode takes leaf-blocked W and Y", MXB_ERR_UNSUPPORTED);
     bool realloc = false;
     for (int i = 0; i < np; ++i) {
         if (nr[i] < 1 || !W[i] || !Y[i]) return batch_fail("bad operand or nrhs in batch");
@@ -1690,6 +1890,14 @@ int Batch::evaluate(const double *const *W, double *const *Y, const int *nrhs, i
             tuned[nr] = bn;
         }
         if (debug_flags & (MXB_DEBUG_CHAIN_LEVELS | MXB_DEBUG_STALL_LEVEL)) chain_all(bn);
+        if (one_launch) {
+            // one tile for the whole launch: the first tensor-core op's width, 64 or 128
+            int w = 0;
+            for (size_t k = 0; k < ops.size() && !w; ++k)
+                if (ops[k].phase != PH_SPLITW) w = tile_width(bn[k]) >= 128 ? 128 : 64;
+            for (size_t k = 0; k < ops.size(); ++k)
+                if (ops[k].phase != PH_SPLITW) bn[k] = w;
+        }
         e.bn = bn;
         int rc = units_for(e, bn, stream);
         if (rc) {
@@ -1781,7 +1989,7 @@ int Batch::profile(const double *const *W, double *const *Y, const int *nrhs, cu
         o.level = m.level;
         o.width = tile_width(e->bn[k]);
         o.pair = tile_pair(e->bn[k]) ? 1 : 0;
-        o.chained = (m.phase != PH_SPLITW && (e->bn[k] & TILE_CHAIN)) ? 1 : 0;
+        o.chained = one_launch ? (k > 0) : ((m.phase != PH_SPLITW && (e->bn[k] & TILE_CHAIN)) ? 1 : 0);
         o.units = e->unit_count[k];
         const double products = m.P == 2 ? 3.0 : 6.0;
         const int tile_rows = o.pair ? 256 : 128;
@@ -2059,6 +2267,8 @@ int Plan::run_split_bf16(const std::vector<Launch> &L, const double *dW, double 
         set_error("the adjoint runs in FP64 mode only (create an FP64 plan for mxb_plan_adjoint)");
         return MXB_ERR_UNSUPPORTED;
     }
+    const int rc = batch_set_one_launch(bf16->self, (debug_flags & MXB_DEBUG_ONE_LAUNCH) != 0);
+    if (rc) return rc;
     return bf16->self->evaluate(&dW, &dY, &nrhs, accumulate, stream, debug_flags, debug_wait_cycles, order);
 }
 
@@ -2074,6 +2284,7 @@ int split_bf16_prepare() { return configure_all_tc() == cudaSuccess ? MXB_OK : M
 int launch_count(const Batch *b)
 {
     if (!b) return 0;
+    if (b->one_launch) return 1;
     int n = (int)b->ops.size();
     if (!b->entries.empty()) {
         const std::vector<int> &bn = b->entries.back().bn;
@@ -2159,6 +2370,17 @@ int batch_status(Batch *b)
 void batch_destroy(Batch *b) { delete b; }
 
 int batch_launches(const Batch *b) { return launch_count(b); }
+
+int batch_set_one_launch(Batch *b, int on)
+{
+    if (!b) return batch_fail("null batch");
+    if (b->one_launch != (on != 0)) {
+        b->one_launch = on != 0;
+        b->clear();
+        b->tuned.clear();
+    }
+    return MXB_OK;
+}
 
 int batch_tuned_widths(const Batch *b, int *widths, int cap)
 {

@@ -91,6 +91,15 @@ __device__ __forceinline__ bool wait_counter(const int *ctr, int target, volatil
     return true;
 }
 
+// Acquire (GPU scope) of a counter another thread of this warp has seen complete: orders this
+// thread's later loads after the writes that the counter's releases published.
+__device__ __forceinline__ void acquire_counter(const int *ctr)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(ctr) : "memory");
+    (void)v;
+}
+
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
 {
     asm volatile(

@@ -445,6 +445,12 @@ class Batch:
         check(_lib.load().mxb_batch_create(arr, len(self.plans), ctypes.byref(h)), "mxb_batch_create")
         self._h = h
 
+    def set_one_launch(self, on: bool = True) -> None:
+        """Evaluate the whole batch as one launch with device-side level barriers
+        (MXB_BATCH_ONE_LAUNCH), or as a sequence of level launches (the default)."""
+        mode = _lib.BATCH_ONE_LAUNCH if on else _lib.BATCH_LEVEL_LAUNCHES
+        check(_lib.load().mxb_batch_set_launch_mode(self._h, mode), "mxb_batch_set_launch_mode")
+
     def close(self):
         if getattr(self, "_h", None):
             _lib.load().mxb_batch_destroy(self._h)

@@ -148,3 +148,35 @@ def test_batch_mixes_split_modes(torch):
         assert 1e-12 < err <= (5e-6 if m != "split_bf16" else 1e-5), (m, err)
         alone = p.evaluate(tw, r).cpu().numpy()
         assert np.linalg.norm(alone - o.cpu().numpy()) <= 1e-6 * np.linalg.norm(want), m
+
+
+def test_one_launch_batch(torch):
+    """MXB_BATCH_ONE_LAUNCH: the W split and every level of every plan (mixed split modes
+    included) run as ONE launch with device-side level barriers; the results match the oracle
+    and the level-launch evaluation of the same batch."""
+    cases = make_cases(5, seed=11)
+    modes = ["split_bf16", "split_bf16_far6", "split_bf16", "split_bf16_x6", "split_bf16"]
+    plans = [H.Plan(c, m) for (c, _), m in zip(cases, modes)]
+    TWs, wants = [], []
+    for k, (c, r) in enumerate(cases):
+        TW = np.random.default_rng(40 + k).standard_normal(c.n * r)
+        TWs.append(torch.as_tensor(TW, device="cuda"))
+        wants.append(O.eval_h2b(c, TW, r))
+    nrhs = [r for _, r in cases]
+    levels = H.Batch(plans)
+    ref = [o.clone() for o in levels.evaluate(TWs, nrhs)]
+    levels.status()
+    one = H.Batch(plans)
+    one.set_one_launch(True)
+    for rep in range(2):  # the second evaluation replays the captured graph
+        outs = one.evaluate(TWs, nrhs)
+        one.status()
+        for m, o, y, want in zip(modes, outs, ref, wants):
+            err = np.linalg.norm(o.cpu().numpy() - want) / np.linalg.norm(want)
+            assert 1e-12 < err <= (5e-6 if m != "split_bf16" else 1e-5), (rep, m, err)
+            assert torch.linalg.norm(o - y).item() <= 1e-6 * np.linalg.norm(want), (rep, m)
+    assert one.info()["launches"] == 1 < levels.info()["launches"]
+    recs = one.profile(TWs, nrhs, [torch.zeros_like(t) for t in TWs])
+    one.status()
+    assert sum(not x["chained"] for x in recs) == 1
+    assert sum(x["flops"] for x in recs) == sum(c.flops(r) for c, r in cases)

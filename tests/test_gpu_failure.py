@@ -97,3 +97,29 @@ def test_level_barrier_that_runs_out_reports_timeout(torch, small_cases):
     got = plan.evaluate(tw, r).cpu().numpy()
     plan.status()
     assert np.linalg.norm(got - want) / np.linalg.norm(want) <= 1e-5
+
+
+def test_one_launch_plan_and_its_level_barrier(torch, small_cases):
+    """A plan evaluated as one launch (test hook MXB_DEBUG_ONE_LAUNCH) matches its ordinary
+    evaluation; with MXB_DEBUG_STALL_LEVEL added, the first level never reports done, the
+    next level's bounded wait runs out, MXB_ERR_TIMEOUT is reported, and the plan recovers."""
+    cds = small_cases["h2b"]
+    r = 96
+    TW = np.random.default_rng(6).standard_normal(cds.n * r)
+    want = O.eval_h2b(cds, TW, r)
+    tw = torch.as_tensor(TW, device="cuda")
+    plan = H.Plan(cds, "split_bf16")
+    plan.set_test_hooks(_lib.DEBUG_ONE_LAUNCH)
+    got = plan.evaluate(tw, r).cpu().numpy()
+    plan.status()
+    assert plan.info()["launches"] == 1
+    assert np.linalg.norm(got - want) / np.linalg.norm(want) <= 1e-5
+    plan.set_test_hooks(_lib.DEBUG_ONE_LAUNCH | _lib.DEBUG_STALL_LEVEL, wait_cycles=100_000_000)
+    plan.evaluate(tw, r)
+    with pytest.raises(_lib.MxbError) as e:
+        plan.status()
+    assert e.value.code == _lib.MXB_ERR_TIMEOUT
+    plan.set_test_hooks(0)
+    again = plan.evaluate(tw, r).cpu().numpy()
+    plan.status()
+    assert np.linalg.norm(again - want) / np.linalg.norm(want) <= 1e-5
