@@ -7,12 +7,15 @@
 // near-field row (several D_xy * W_y) or a transfer (two child projections) is one
 // pipeline with one epilogue and no atomics: every output tile has exactly one writer.
 //
-// Shared-memory layout per stage: A tile as [k][m] (m contiguous, row pitch 72 doubles)
-// and B tile as [n][k] (k contiguous, pitch 20 doubles).  The pitches make both DMMA
-// fragment reads (A: 8 rows x 4 k per warp, B: 4 k x 8 cols) hit every bank pair exactly
-// twice, the 2-wavefront minimum of a 256-byte warp load.
+// Shared-memory layout per stage: A tile as [k][m] (m contiguous, row pitch 72 doubles), or,
+// for a transposed A (whose K is contiguous in memory), as [m][k] (pitch 20); B tile as [n][k]
+// (k contiguous, pitch 20 doubles).  The pitches make the DMMA fragment reads (A: 8 rows x 4 k
+// per warp, B: 4 k x 8 cols) hit every bank pair exactly twice, the 2-wavefront minimum of a
+// 256-byte warp load.  Global -> shared copies move pairs of doubles along the contiguous
+// dimension as one 16-byte cp.async where the block is 16-byte aligned with an even leading
+// dimension, single doubles otherwise.
 //
-// Occupancy: 4 CTAs (16 warps) per SM at <= 128 registers and 39 KB of shared memory each.
+// Occupancy: 4 CTAs (16 warps) per SM at <= 128 registers and 40 KB of shared memory each.
 // Measured at N = 65536 / 1024 rhs this is 2.4 % faster than 3 CTAs with 3 stages (160
 // registers); 5 or 6 CTAs per SM gain nothing more (the DMMA pipe is the limit).
 #include <cstdio>
@@ -25,7 +28,8 @@ namespace {
 constexpr int BM = 64, BN = 64, BK = 16, STAGES = 2, THREADS = 128;
 constexpr int A_LD = BM + 8;
 constexpr int B_LD = BK + 4;
-constexpr int A_TILE = BK * A_LD;
+constexpr int T_LD = BK + 4;  // transposed A operand: [m][k], k contiguous, like B
+constexpr int A_TILE = (BK * A_LD > BM * T_LD) ? BK * A_LD : BM * T_LD;
 constexpr int B_TILE = BN * B_LD;
 constexpr int STAGE = A_TILE + B_TILE;
 constexpr size_t SMEM_BYTES = size_t(STAGES) * STAGE * sizeof(double);
@@ -60,6 +64,7 @@ struct Loader {
     int k0;
     int q;
     bool a16, b16;  // pairs of doubles along the contiguous dimension are 16-byte aligned
+    bool t16;       // the same for a transposed A (pairs along K)
 };
 
 __device__ __forceinline__ const double *operand_ptr(const Operands &ops, int kind, int64_t row)
@@ -87,6 +92,7 @@ __device__ __forceinline__ void load_item(Loader &L, const Item *items, const Op
     // tile rows m0 and K offsets k0 are even, so every pair starts 16-byte aligned when the
     // block does and its leading dimension is even
     L.a16 = !it.trans && ((reinterpret_cast<uintptr_t>(L.A) & 15) == 0) && !(it.lda & 1);
+    L.t16 = it.trans && ((reinterpret_cast<uintptr_t>(L.A) & 15) == 0) && !(it.lda & 1);
     L.b16 = ((reinterpret_cast<uintptr_t>(L.B) & 15) == 0) && !(it.ldb & 1);
 }
 
@@ -108,11 +114,14 @@ gemm_f64_kernel(const Task *__restrict__ tasks, const Item *__restrict__ items, 
     L.q = 0;
     if (t.nitem > 0) load_item(L, titems, ops);
 
+    // bit s: stage s holds a transposed A tile, in the [m][k] layout
+    int trmask = 0;
     auto issue = [&](int stage) {
         while (L.k0 >= L.K) {  // next item with work (items with K == 0 are skipped)
             ++L.q;
             load_item(L, titems, ops);
         }
+        trmask = L.trans ? (trmask | (1 << stage)) : (trmask & ~(1 << stage));
         double *As = smem + stage * STAGE;
         double *Bs = As + A_TILE;
         const int k0 = L.k0;
@@ -135,6 +144,16 @@ gemm_f64_kernel(const Task *__restrict__ tasks, const Item *__restrict__ items, 
                 const double *src = v ? L.A + (size_t)(t.m0 + m) + (size_t)(k0 + k) * L.lda : L.A;
                 cp_async8(As + k * A_LD + m, src, v);
             }
+        } else if (L.t16) {
+            // transposed A: K is contiguous in memory; kept [m][k] so K pairs move as 16 bytes
+#pragma unroll
+            for (int i = 0; i < (BM * BK) / (2 * THREADS); ++i) {
+                const int idx = tid + i * THREADS;
+                const int k = (idx & (BK / 2 - 1)) * 2, m = idx / (BK / 2);
+                const int nv = (t.m0 + m < t.M) ? max(0, min(2, L.K - (k0 + k))) : 0;
+                const double *src = nv ? L.A + (size_t)(k0 + k) + (size_t)(t.m0 + m) * L.lda : L.A;
+                cp_async16(As + m * T_LD + k, src, nv * 8);
+            }
         } else {
 #pragma unroll
             for (int i = 0; i < (BM * BK) / THREADS; ++i) {
@@ -142,7 +161,7 @@ gemm_f64_kernel(const Task *__restrict__ tasks, const Item *__restrict__ items, 
                 const int k = idx & (BK - 1), m = idx / BK;
                 const bool v = (t.m0 + m < t.M) && (k0 + k < L.K);
                 const double *src = v ? L.A + (size_t)(k0 + k) + (size_t)(t.m0 + m) * L.lda : L.A;
-                cp_async8(As + k * A_LD + m, src, v);
+                cp_async8(As + m * T_LD + k, src, v);
             }
         }
         if (L.b16) {
@@ -188,12 +207,18 @@ gemm_f64_kernel(const Task *__restrict__ tasks, const Item *__restrict__ items, 
 
         const double *As = smem + (kt % STAGES) * STAGE;
         const double *Bs = As + A_TILE;
+        const bool tr = (trmask >> (kt % STAGES)) & 1;
 #pragma unroll
         for (int kk = 0; kk < BK / 4; ++kk) {
             double a[4], b[4];
             const int kr = kk * 4 + (lane & 3);
+            if (tr) {
 #pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = As[kr * A_LD + wm * 32 + i * 8 + (lane >> 2)];
+                for (int i = 0; i < 4; ++i) a[i] = As[(wm * 32 + i * 8 + (lane >> 2)) * T_LD + kr];
+            } else {
+#pragma unroll
+                for (int i = 0; i < 4; ++i) a[i] = As[kr * A_LD + wm * 32 + i * 8 + (lane >> 2)];
+            }
 #pragma unroll
             for (int j = 0; j < 4; ++j) b[j] = Bs[(wn * 32 + j * 8 + (lane >> 2)) * B_LD + kr];
 #pragma unroll
