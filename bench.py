@@ -678,6 +678,11 @@ def main():
                 whole_evaluation_tflops=round((flops if best == "fp64" else exec_flops[best]) / (ms * 1e-3) / 1e12, 3))
     roof["frac"] = round(roof["achieved"] / roof["peak"], 4)
     roof["traffic"] = traffic
+    small = profile_traffic().get("small_case")
+    if traffic is None and small:
+        roof["traffic_small_case"] = {"n": small["n"], "bytes_per_launch": round(
+            small["tc_gemm_dram_bytes_per_evaluation"] / small["tc_gemm_launches_per_evaluation"]),
+            "note": "measured at N=32768 (profiles/traffic.json); not scaled to this size"}
 
     # end to end through the reference-signature drop-in, host buffers (pinned)
     e2e = None
