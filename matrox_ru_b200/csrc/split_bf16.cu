@@ -308,7 +308,8 @@ struct TcCfg {
     // and epilogue warps in a pair)
     static constexpr int RING_READERS = PAIR ? 2 * (1 + EPI_WARPS) + 1 : 1 + EPI_WARPS;
     static constexpr int THREADS = (EPI_WARPS + 2) * 32;
-    static constexpr int UNIT_WRITERS = EPI_WARPS * (PAIR ? 2 : 1);  // epilogue warps per unit
+    // level-count increments per unit: one per CTA (its last epilogue warp to finish the unit)
+    static constexpr int UNIT_WRITERS = PAIR ? 2 : 1;
     static constexpr int COLS = BN / 2;          // accumulator columns per epilogue thread
     // old values loaded ahead of the stores in the epilogue's read-modify-writes (fewer where
     // 128 accumulators already fill the registers)
@@ -365,6 +366,9 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
     volatile int *ring_kt = ring + RING;  // K tiles of the unit in ring slot i
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(const_cast<int *>(ring_kt) + RING);
     volatile int *abort_word = reinterpret_cast<volatile int *>(tmem_slot + 1);
+    // chained launches: epilogue warps done with the unit of sequence number q, at q % (2 RING)
+    // (the last of them raises the level count once for the CTA)
+    unsigned *unit_warps = reinterpret_cast<unsigned *>(const_cast<int *>(abort_word) + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t rank = PAIR ? tc::cluster_ctarank() : 0u;
@@ -423,6 +427,7 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
             tc::mbar_init(&uempty[i], C::RING_READERS);
         }
         *abort_word = 0;
+        for (int i = 0; i < 2 * RING; ++i) unit_warps[i] = 0;
         tc::fence_mbar_init();
     }
     if (warp == 0) {
@@ -992,12 +997,24 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
             }
             if (la.nlevels > 1) {
                 // this warp's part of the unit is stored: make it visible (also to the bulk
-                // copies of later levels) and count the warp done for the unit's level
+                // copies of later levels); the CTA's last warp to get here counts the unit done
+                // for its level (one global atomic per unit and CTA, not per warp: the counters
+                // of a level are hit by every unit of the level)
                 asm volatile("fence.proxy.async.global;\n" ::: "memory");
                 __threadfence();
                 __syncwarp();
-                const int lvl = (un.chain >> 20) & 0xFF;
-                if (lane == 0 && !(la.stall_level && lvl == 0)) atomicAdd(la.level_done + lvl, 1);
+                if (lane == 0) {
+                    // a warp can run at most RING units ahead of the slowest (the producer
+                    // refills a ring slot only after every reader has taken its unit), so
+                    // 2 RING counters never alias
+                    unsigned *cnt = &unit_warps[(slot - 1) % (2 * RING)];
+                    if (atomicAdd(cnt, 1u) == (unsigned)(C::EPI_WARPS - 1)) {
+                        atomicExch(cnt, 0u);
+                        __threadfence();
+                        const int lvl = (un.chain >> 20) & 0xFF;
+                        if (!(la.stall_level && lvl == 0)) atomicAdd(la.level_done + lvl, 1);
+                    }
+                }
             }
         }
     }
