@@ -937,18 +937,27 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                 const double *src = pa->W + pa->wofs[t.c_row];
                 uint8_t *base = pa->buf[t.t_buf] + ((size_t)t.out_kt * pa->NT + (size_t)nt * KTv) * 3 * (size_t)TILE_BYTES;
                 const int tid = threadIdx.x;  // the epilogue warps are warps 0 .. EPI_WARPS - 1
+                constexpr int PER = 1024 / (C::EPI_WARPS * 32);  // 16-byte chunks per thread and K tile
                 for (int kt = 0; kt < KTv; ++kt) {
-                    for (int idx = tid; idx < 1024; idx += C::EPI_WARPS * 32) {
-                        const int c = idx % 8, rr = idx / 8;
-                        const int n = nt * 128 + rr;
-                        __nv_bfloat16 h[8], m[8], l[8];
+                    // all of the thread's loads of the K tile in flight before any split
+                    double x[PER][8];
+#pragma unroll
+                    for (int i = 0; i < PER; ++i) {
+                        const int idx = tid + i * C::EPI_WARPS * 32;
+                        const int c = idx % 8, n = nt * 128 + idx / 8;
 #pragma unroll
                         for (int e = 0; e < 8; ++e) {
                             const int k = kt * 64 + c * 8 + e;
-                            const double x = (n < nrhs && k < t.M) ? src[k + (size_t)n * t.ldc] : 0.0;
-                            tc::split3(x, h[e], m[e], l[e]);
+                            x[i][e] = (n < nrhs && k < t.M) ? src[k + (size_t)n * t.ldc] : 0.0;
                         }
-                        store_parts(base + (size_t)kt * 3 * TILE_BYTES, 3, rr, c, h, m, l);
+                    }
+#pragma unroll
+                    for (int i = 0; i < PER; ++i) {
+                        const int idx = tid + i * C::EPI_WARPS * 32;
+                        __nv_bfloat16 h[8], m[8], l[8];
+#pragma unroll
+                        for (int e = 0; e < 8; ++e) tc::split3(x[i][e], h[e], m[e], l[e]);
+                        store_parts(base + (size_t)kt * 3 * TILE_BYTES, 3, idx / 8, idx % 8, h, m, l);
                     }
                 }
             } else {
@@ -1441,8 +1450,9 @@ int Batch::units_for(Entry &e, const std::vector<int> &bn, cudaStream_t stream)
             if (prev > 0xFFFFF) return batch_fail("a level of the one-launch evaluation has too many units");
             const int32_t chain = ((int32_t)k << 20) | prev;
             if (m.phase == PH_SPLITW) {
+                // the 128-column tiles that the launch's units read (its tile is 64 or 128 wide)
                 for (int t = split_task0; t < split_task0 + split_tasks; ++t) {
-                    const int NT = plans[tasks[t].plan]->bf16->nt_cap;
+                    const int NT = (int)ceil_div(e.nrhs[tasks[t].plan], 128);
                     for (int nt = 0; nt < NT; ++nt) units.push_back(TcUnit{t, nt, 0, chain | (3 << 28)});
                 }
             } else {
