@@ -131,6 +131,12 @@ def batched_report(args, count=64, seed=20261204):
     one.status()
     errs1 = [float(torch.linalg.norm(o - y) / torch.linalg.norm(y)) for o, y in zip(outs1, refs)]
     one_launches = one.info()["launches"]
+    # each level's span inside the one launch (the kernel's own timer), and the level launches
+    one_levels = [[x["phase"], x["level"], round(x["level_ms"], 4)] for x in one.profile(TWs, nrhs, outs1)]
+    one.status()
+    multi_launches = [[x["phase"], x["level"], x["width"], "chained" if x["chained"] else "launch", round(x["ms"], 4)]
+                      for x in batch.profile(TWs, nrhs, outs)]
+    batch.status()
     del one, outs1
     single_ms = 0.0
     for p, t, r, o in zip(plans, TWs, nrhs, outs):
@@ -141,7 +147,8 @@ def batched_report(args, count=64, seed=20261204):
             "batch_ms": round(batch_ms, 3), "sum_of_single_plan_ms": round(single_ms, 3),
             "one_launch": {"ms": round(one_ms, 3), "launches": one_launches,
                            "tflops": round(flops / (one_ms * 1e-3) / 1e12, 2),
-                           "max_rel_err_vs_fp64_same_cds": max(errs1)},
+                           "max_rel_err_vs_fp64_same_cds": max(errs1), "levels_ms": one_levels},
+            "level_launches_ms": multi_launches,
             "batch_tflops": round(flops / (batch_ms * 1e-3) / 1e12, 2),
             "launches_per_batch_evaluation": info["launches"],
             "launches_single_plans": sum(p.info()["launches"] for p in plans),

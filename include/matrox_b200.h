@@ -347,6 +347,9 @@ typedef struct mxb_op_profile {
     int32_t chained;      /* 1: ran inside the launch of the record before it, as a later tree
                              level that waits on the device for the level before; ms is 0 and
                              that launch's ms covers both */
+    float level_ms;       /* one-launch batches: this level's span inside the launch, from the
+                             kernel's own timer (last unit of the level before to its own last
+                             unit written); 0 elsewhere */
 } mxb_op_profile;
 /* `*nops` receives the number of launches; at most `cap` records are written. */
 MXB_API int32_t mxb_plan_profile(mxb_plan *plan, const double *dW, double *dY, int32_t nrhs, void *stream,

@@ -65,7 +65,7 @@ class CdsDesc(ctypes.Structure):
 class OpProfile(ctypes.Structure):
     _fields_ = [("phase", I32), ("level", I32), ("width", I32), ("units", I32),
                 ("flops", ctypes.c_double), ("issued_flops", ctypes.c_double), ("ms", ctypes.c_float),
-                ("pair", I32), ("chained", I32)]
+                ("pair", I32), ("chained", I32), ("level_ms", ctypes.c_float)]
 
 
 _REF_ARGS_H2B = [P] * 12 + [I32] + [P] * 9 + [P] * 8  # up to fpairy

@@ -156,6 +156,9 @@ struct LaunchArgs {
     int nlevels;            // chained levels (1: none); a unit's level is in TcUnit::chain
     int *level_done;        // per level: epilogue warps done with a unit of it (zero at launch)
     int stall_level;        // test hook: level 0 never reports done, so level 1's waits run out
+    // profiling of chained launches (null otherwise): [0] the earliest CTA start, [1 + j] the
+    // time the last unit of level j was written (%globaltimer, ns)
+    unsigned long long *level_ns;
 };
 
 // ---------------------------------------------------------------------------------------
@@ -439,6 +442,7 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
     if constexpr (PAIR) tc::cluster_sync();  // both CTAs' barriers and TMEM exist
     tc::fence_after_sync();
     const uint32_t tmem = *tmem_slot;
+    if (la.level_ns && threadIdx.x == 0) atomicMin(la.level_ns, tc::globaltimer_ns());
 
     if (warp == C::EPI_WARPS) {
         if (lane == 0) {
@@ -1022,6 +1026,7 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                         __threadfence();
                         const int lvl = (un.chain >> 20) & 0xFF;
                         if (!(la.stall_level && lvl == 0)) atomicAdd(la.level_done + lvl, 1);
+                        if (la.level_ns) atomicMax(la.level_ns + 1 + lvl, tc::globaltimer_ns());
                     }
                 }
             }
@@ -1239,6 +1244,7 @@ struct Batch : public mxb_batch {
     // launch of the kernel with 3-part stages (OUT_SPLIT tasks at [split_task0, + split_tasks)).
     bool one_launch = false;
     int split_task0 = 0, split_tasks = 0;
+    unsigned long long *level_ns = nullptr;  // while profiling a one-launch evaluation
     std::vector<SplitJob> jobs;
     TcTask *dTasks = nullptr;
     TcItem *dItems = nullptr;
@@ -1584,6 +1590,7 @@ int Batch::enqueue(Entry &e, cudaStream_t stream, int debug_flags, long long wai
         a.nlevels = (int)ops.size();
         a.level_done = dLevel;
         a.stall_level = (debug_flags & MXB_DEBUG_STALL_LEVEL) != 0;
+        a.level_ns = level_ns;
         // 128 columns: the slot-ring kernel (bf16x3 units hold two slots, bf16x6 units three)
         const cudaError_t err = w == 128 && slots_enabled() ? launch_tc_slots(a, stream)
                                                             : launch_tc(3, w, false, false, a, stream);
@@ -2098,7 +2105,19 @@ int Batch::profile(const double *const *W, double *const *Y, const int *nrhs, cu
     int rc = MXB_OK;
     for (cudaEvent_t &x : ev)
         if (!rc && cudaEventCreate(&x) != cudaSuccess) rc = batch_fail("profile: creating CUDA events failed", MXB_ERR_CUDA);
+    // one launch: each level's span on the device, from the kernel's own timestamps
+    std::vector<unsigned long long> lns(ops.size() + 1, 0);
+    if (!rc && one_launch) {
+        if (cudaMalloc(&level_ns, lns.size() * sizeof(unsigned long long)) != cudaSuccess) {
+            level_ns = nullptr;
+            rc = batch_fail("profile: level timer allocation failed", MXB_ERR_NOMEM);
+        }
+    }
     for (int rep = 0; rep < 2 && !rc; ++rep) {
+        if (level_ns) {
+            cudaMemsetAsync(level_ns, 0, lns.size() * sizeof(unsigned long long), stream);
+            cudaMemsetAsync(level_ns, 0xff, sizeof(unsigned long long), stream);  // start: minimum of
+        }
         cudaEventRecord(ev[0], stream);
         for (size_t k = 0; k < ops.size() && !rc; ++k) {
             rc = enqueue(*e, stream, 0, 0, e->bn, (int)k);
@@ -2106,6 +2125,13 @@ int Batch::profile(const double *const *W, double *const *Y, const int *nrhs, cu
         }
         if (!rc && cudaStreamSynchronize(stream) != cudaSuccess)
             rc = batch_fail("profile: stream synchronisation failed", MXB_ERR_CUDA);
+    }
+    if (level_ns) {
+        if (!rc && cudaMemcpy(lns.data(), level_ns, lns.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost) !=
+                       cudaSuccess)
+            rc = batch_fail("profile: reading the level timers failed", MXB_ERR_CUDA);
+        cudaFree(level_ns);
+        level_ns = nullptr;
     }
     if (nops) *nops = (int)ops.size();
     std::vector<TcUnit> units;
@@ -2139,6 +2165,8 @@ int Batch::profile(const double *const *W, double *const *Y, const int *nrhs, cu
         }
         cudaEventElapsedTime(&o.ms, ev[k], ev[k + 1]);
         if (o.chained) o.ms = 0.f;
+        if (one_launch && lns[k + 1] >= lns[k] && lns[0] != ~0ull)
+            o.level_ms = (float)((double)(lns[k + 1] - (k ? lns[k] : lns[0])) * 1e-6);
     }
     for (cudaEvent_t x : ev)
         if (x) cudaEventDestroy(x);

@@ -91,6 +91,13 @@ __device__ __forceinline__ bool wait_counter(const int *ctr, int target, volatil
     return true;
 }
 
+__device__ __forceinline__ unsigned long long globaltimer_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+    return t;
+}
+
 // Acquire (GPU scope) of a counter another thread of this warp has seen complete: orders this
 // thread's later loads after the writes that the counter's releases published.
 __device__ __forceinline__ void acquire_counter(const int *ctr)

@@ -203,7 +203,7 @@ def cds_desc(cds, keep: list) -> _lib.CdsDesc:
 def _profile_records(recs, n):
     return [{"phase": _lib.PHASES.get(r.phase, str(r.phase)), "level": r.level, "width": r.width, "units": r.units,
              "pair": bool(r.pair), "chained": bool(r.chained), "flops": r.flops, "issued_flops": r.issued_flops,
-             "ms": r.ms} for r in recs[:min(n, len(recs))]]
+             "ms": r.ms, "level_ms": r.level_ms} for r in recs[:min(n, len(recs))]]
 
 
 def kernel_blocks(cds, X, kernel, stream=None):

@@ -180,3 +180,6 @@ def test_one_launch_batch(torch):
     one.status()
     assert sum(not x["chained"] for x in recs) == 1
     assert sum(x["flops"] for x in recs) == sum(c.flops(r) for c, r in cases)
+    # every level's own span, from the kernel's timer, inside the launch's event time
+    assert all(x["level_ms"] > 0.0 for x in recs)
+    assert sum(x["level_ms"] for x in recs) <= 1.05 * recs[0]["ms"]
