@@ -744,6 +744,7 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
         const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
         const uint32_t acce0 = PAIR ? tc::peer_smem(&acce[0], 0) : tc::smem_u32(&acce[0]);
         uint32_t g = 0, slot = 0;
+        int ewaited = 0;  // last chained level this warp acquired
         for (;;) {
             int u = 0, ktiles = 0;
             if (lane == 0) u = take_unit(slot, ktiles);
@@ -757,12 +758,13 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
             const TcTask t = la.tasks[un.task];
             const int kc = unit_kchain(unit_parts(un.chain));
             const int fills = (ktiles + kc - 1) / kc;
-            if (la.nlevels > 1 && ((un.chain >> 20) & 0xFF) > 0) {
+            if (la.nlevels > 1 && ((un.chain >> 20) & 0xFF) > ewaited) {
                 // the old values this unit reads back (Y, the far result) may come from an
                 // earlier level of this launch: acquire that level's completion here too (the
-                // producer's wait covers only its bulk copies).  Lane 0 waits; then every lane
-                // takes its own acquire of the completed count.
+                // producer's wait covers only its bulk copies), once per level and warp.  Lane 0
+                // waits; then every lane takes its own acquire of the completed count.
                 const int lvl = (un.chain >> 20) & 0xFF;
+                ewaited = lvl;
                 const int *ctr = la.level_done + lvl - 1;
                 int done = 1;
                 if (lane == 0)
