@@ -311,8 +311,8 @@ struct TcCfg {
     // and epilogue warps in a pair)
     static constexpr int RING_READERS = PAIR ? 2 * (1 + EPI_WARPS) + 1 : 1 + EPI_WARPS;
     static constexpr int THREADS = (EPI_WARPS + 2) * 32;
-    // level-count increments per unit: one per CTA (its last epilogue warp to finish the unit)
-    static constexpr int UNIT_WRITERS = PAIR ? 2 : 1;
+    // level-count increments per unit: one per epilogue warp (of both CTAs of a pair)
+    static constexpr int UNIT_WRITERS = EPI_WARPS * (PAIR ? 2 : 1);
     static constexpr int COLS = BN / 2;          // accumulator columns per epilogue thread
     // old values loaded ahead of the stores in the epilogue's read-modify-writes (fewer where
     // 128 accumulators already fill the registers)
@@ -369,9 +369,6 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
     volatile int *ring_kt = ring + RING;  // K tiles of the unit in ring slot i
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(const_cast<int *>(ring_kt) + RING);
     volatile int *abort_word = reinterpret_cast<volatile int *>(tmem_slot + 1);
-    // chained launches: epilogue warps done with the unit of sequence number q, at q % (2 RING)
-    // (the last of them raises the level count once for the CTA)
-    unsigned *unit_warps = reinterpret_cast<unsigned *>(const_cast<int *>(abort_word) + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t rank = PAIR ? tc::cluster_ctarank() : 0u;
@@ -430,7 +427,7 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
             tc::mbar_init(&uempty[i], C::RING_READERS);
         }
         *abort_word = 0;
-        for (int i = 0; i < 2 * RING; ++i) unit_warps[i] = 0;
+
         tc::fence_mbar_init();
     }
     if (warp == 0) {
@@ -745,6 +742,21 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
         const uint32_t acce0 = PAIR ? tc::peer_smem(&acce[0], 0) : tc::smem_u32(&acce[0]);
         uint32_t g = 0, slot = 0;
         int ewaited = 0;  // last chained level this warp acquired
+        // Chained launches: this warp's finished units of level pend_level not yet counted.  They
+        // are counted (after one fence for all their stores) when the warp takes its first unit
+        // of a later level, or at the end: one fence and one atomic per level and warp.
+        int pend_level = 0, pend = 0;
+        auto flush = [&]() {
+            if (!pend) return;
+            asm volatile("fence.proxy.async.global;\n" ::: "memory");
+            __threadfence();
+            __syncwarp();
+            if (lane == 0) {
+                if (!(la.stall_level && pend_level == 0)) atomicAdd(la.level_done + pend_level, pend);
+                if (la.level_ns) atomicMax(la.level_ns + 1 + pend_level, tc::globaltimer_ns());
+            }
+            pend = 0;
+        };
         for (;;) {
             int u = 0, ktiles = 0;
             if (lane == 0) u = take_unit(slot, ktiles);
@@ -752,9 +764,14 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
             ktiles = __shfl_sync(0xffffffffu, ktiles, 0);
             if (u < 0) {
                 if (u == -2 && lane == 0) raise_abort();
+                if (u == -1) flush();
                 break;
             }
             const TcUnit un = la.units[u];
+            if (la.nlevels > 1 && ((un.chain >> 20) & 0xFF) != pend_level) {
+                flush();
+                pend_level = (un.chain >> 20) & 0xFF;
+            }
             const TcTask t = la.tasks[un.task];
             const int kc = unit_kchain(unit_parts(un.chain));
             const int fills = (ktiles + kc - 1) / kc;
@@ -1010,28 +1027,7 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                     }
                 }
             }
-            if (la.nlevels > 1) {
-                // this warp's part of the unit is stored: make it visible (also to the bulk
-                // copies of later levels); the CTA's last warp to get here counts the unit done
-                // for its level (one global atomic per unit and CTA, not per warp: the counters
-                // of a level are hit by every unit of the level)
-                asm volatile("fence.proxy.async.global;\n" ::: "memory");
-                __threadfence();
-                __syncwarp();
-                if (lane == 0) {
-                    // a warp can run at most RING units ahead of the slowest (the producer
-                    // refills a ring slot only after every reader has taken its unit), so
-                    // 2 RING counters never alias
-                    unsigned *cnt = &unit_warps[(slot - 1) % (2 * RING)];
-                    if (atomicAdd(cnt, 1u) == (unsigned)(C::EPI_WARPS - 1)) {
-                        atomicExch(cnt, 0u);
-                        __threadfence();
-                        const int lvl = (un.chain >> 20) & 0xFF;
-                        if (!(la.stall_level && lvl == 0)) atomicAdd(la.level_done + lvl, 1);
-                        if (la.level_ns) atomicMax(la.level_ns + 1 + lvl, tc::globaltimer_ns());
-                    }
-                }
-            }
+            if (la.nlevels > 1) ++pend;  // counted when the warp moves past this level
         }
     }
     __syncwarp();
