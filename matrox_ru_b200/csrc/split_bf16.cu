@@ -385,17 +385,20 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
     auto arrive_local = [&](uint64_t *bar) {
         asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(tc::smem_u32(bar)) : "memory");
     };
-    // Next unit of the ring for a reader (one thread): waits for slot `slot`, takes the unit and
-    // its K-tile count and releases the slot to the producer (in the even CTA of a pair).
-    // -2: a wait gave up.
-    auto take_unit = [&](uint32_t &slot, int &ktiles) -> int {
+    // Next unit of the ring for a reader (one thread): waits for slot `slot`, takes the unit,
+    // its K-tile count and its operand parts (published as ktiles | parts << 24, so the MMA
+    // issuer needs no global load per unit), and releases the slot to the producer (in the
+    // even CTA of a pair).  -2: a wait gave up.
+    auto take_unit = [&](uint32_t &slot, int &ktiles, int *parts = nullptr) -> int {
         const int i = (int)(slot % RING);
         const uint32_t parity = (slot / RING) & 1u;
         ++slot;
         int u = -2;
         if (wait_x(&ufull[i], parity, abort_word)) {
             u = ring[i];
-            ktiles = ring_kt[i];
+            const int v = ring_kt[i];
+            ktiles = v & 0xFFFFFF;
+            if (parts) *parts = v >> 24;
         }
         if constexpr (PAIR) {
             if (rank == 1) tc::mbar_arrive_remote(tc::peer_smem(&uempty[i], 0));
@@ -458,7 +461,12 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                     // claim the next unit and publish it to every reader
                     u = atomicAdd(la.next_unit, 1);
                     if (u >= la.nunits) u = -1;
-                    if (u >= 0) kt_unit = la.units[u].ktiles;
+                    int kt_pub = 0;
+                    if (u >= 0) {
+                        const TcUnit cu = la.units[u];
+                        kt_unit = cu.ktiles;
+                        kt_pub = cu.ktiles | (unit_parts(cu.chain) << 24);
+                    }
                     const int i = (int)(slot % RING);
                     const uint32_t round = slot / RING;
                     ++slot;
@@ -467,10 +475,10 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                         break;
                     }
                     ring[i] = u;
-                    ring_kt[i] = kt_unit;
+                    ring_kt[i] = kt_pub;
                     if constexpr (PAIR) {
                         tc::st_remote_u32(tc::peer_smem((const void *)&ring[i], 1), (uint32_t)u);
-                        tc::st_remote_u32(tc::peer_smem((const void *)&ring_kt[i], 1), (uint32_t)kt_unit);
+                        tc::st_remote_u32(tc::peer_smem((const void *)&ring_kt[i], 1), (uint32_t)kt_pub);
                         tc::mbar_arrive_remote(tc::peer_smem(&ufull[i], 1));
                     }
                     arrive_local(&ufull[i]);
@@ -611,13 +619,12 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
             uint32_t vpos = 0;  // VS: slots consumed so far (the producer's allocation order)
             bool any = false, stop = false;
             while (!stop) {
-                int ktiles = 0;
-                const int u = take_unit(slot, ktiles);
+                int ktiles = 0, up = P;
+                const int u = take_unit(slot, ktiles, &up);
                 if (u < 0) {
                     if (u == -2) raise_abort();
                     break;
                 }
-                const int up = ktiles ? unit_parts(la.units[u].chain) : P;
                 const int nprod = up == 2 ? 3 : 6;
                 const int kc = unit_kchain(up);
                 for (int i = 0; i < ktiles; ++i, ++g) {
