@@ -617,6 +617,7 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
             uint32_t ga = 0;    // accumulator-fill counter
             uint32_t slot = 0;  // ring counter
             uint32_t vpos = 0;  // VS: slots consumed so far (the producer's allocation order)
+            const uint32_t smem_base = tc::smem_u32(smem);
             bool any = false, stop = false;
             while (!stop) {
                 int ktiles = 0, up = P;
@@ -646,17 +647,23 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                         tc::fence_after_sync();
                         const uint32_t dst = tmem + (uint32_t)(b * BN);
                         uint32_t accum = first ? 0u : 1u;
+                        // descriptors of the tile's parts, once per tile (the issuing thread's
+                        // work per MMA must stay well under an MMA's duration)
+                        uint64_t dA[3], dB[3];
+#pragma unroll
+                        for (int p = 0; p < 3; ++p) {
+                            const uint32_t sl = (vpos + (uint32_t)p) % C::NSLOT;
+                            const uint32_t base = smem_base + sl * (uint32_t)C::SLOT;
+                            dA[p] = tc::smem_desc_sw128(base);
+                            dB[p] = tc::smem_desc_sw128(base + TILE_BYTES);
+                        }
 #pragma unroll
                         for (int ks = 0; ks < 4; ++ks) {
 #pragma unroll
                             for (int j = 0; j < 6; ++j) {
                                 if (j >= nprod) break;
-                                const uint32_t sa_ = tc::smem_u32(smem + (size_t)((vpos + (uint32_t)PA[j]) % C::NSLOT) * C::SLOT);
-                                const uint32_t sb_ =
-                                    tc::smem_u32(smem + (size_t)((vpos + (uint32_t)PB[j]) % C::NSLOT) * C::SLOT) + TILE_BYTES;
-                                const uint64_t ad = tc::smem_desc_sw128(sa_) + (uint64_t)((ks * 32) >> 4);
-                                const uint64_t bd = tc::smem_desc_sw128(sb_) + (uint64_t)((ks * 32) >> 4);
-                                tc::mma_bf16(dst, ad, bd, IDESC, accum);
+                                tc::mma_bf16(dst, dA[PA[j]] + (uint64_t)(ks * 2), dB[PB[j]] + (uint64_t)(ks * 2), IDESC,
+                                             accum);
                                 accum = 1;
                             }
                         }
