@@ -321,10 +321,6 @@ struct TcCfg {
     static constexpr int NACC = BN >= 256 ? 2 : 4;  // TMEM accumulator buffers (512 columns at most)
     static constexpr int TMEM_COLS = NACC * BN;
     static constexpr int M_MMA = PAIR ? 256 : 128;
-    // slot-ring pipeline (VS): one slot holds one A part and one B part of a K tile, a K tile
-    // takes as many consecutive slots (mod NSLOT) as its operands have parts
-    static constexpr int SLOT = TILE_BYTES + B_ROWS_BYTES;
-    static constexpr int NSLOT = STAGES * STAGE / SLOT;
     static_assert(SMEM <= 232448, "shared memory");
     static_assert(B_ROWS % 64 == 0, "B rows per CTA");
 };
@@ -347,14 +343,11 @@ struct TcCfg {
 // landed" to the even CTA's pfull barrier, its epilogue warps arrive on the even CTA's acce
 // barrier, and the even CTA's commits arrive on both CTAs' barriers.  A failed wait in either
 // CTA sets both CTAs' abort words.
-// VS: the stages are a ring of NSLOT slots shared by K tiles of 2 or 3 parts (launches that
-// mix both, single-CTA only), so 2-part tiles get more tiles in flight than the fixed stages.
-template <int P, int BN, int STAGES_, bool PAIR, bool ORD, bool VS = false>
+template <int P, int BN, int STAGES_, bool PAIR, bool ORD>
 __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_gemm_kernel(LaunchArgs la)
 {
     using C = TcCfg<P, BN, STAGES_, PAIR>;
-    static_assert(!VS || (!PAIR && C::B_ROWS == 128 && C::NSLOT * C::SLOT <= C::STAGES * C::STAGE), "slot ring");
-    constexpr int NB = VS ? C::NSLOT : C::STAGES;  // full / empty barriers (per slot or per stage)
+    constexpr int NB = C::STAGES;  // full / empty / pair barriers: one per stage
     constexpr int RING = C::RING;
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -451,7 +444,6 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
             uint32_t g = 0;               // K-tile counter of this CTA
             uint32_t slot = 0;            // ring counter
             int waited = 0;               // last chained level waited for
-            uint32_t vpos = 0;            // VS: slots allocated so far
             uint32_t filled[C::STAGES];   // rounds filled per stage (drained before exit)
 #pragma unroll
             for (int s = 0; s < C::STAGES; ++s) filled[s] = 0;
@@ -537,33 +529,6 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                         }
                     }
                     for (int kt = 0; kt < it.KT; ++kt, ++g) {
-                        if constexpr (VS) {
-                            // slots pos .. pos + up - 1 (mod NSLOT); slot use = position / NSLOT
-                            bool ok = true;
-                            for (int p = 0; p < up && ok; ++p) {
-                                const uint32_t q = vpos + (uint32_t)p;
-                                ok = wait_x(&empty[q % C::NSLOT], ((q / C::NSLOT) & 1) ^ 1, abort_word);
-                            }
-                            if (!ok) {
-                                raise_abort();
-                                stop = true;
-                                break;
-                            }
-                            if (!(la.stall_test && blockIdx.x == 0 && g == 0)) {  // test hook: never filled
-                                const uint8_t *ga = a_pool + it.a_off + ((size_t)mt * it.KT + kt) * (size_t)up * TILE_BYTES;
-                                const uint8_t *gb =
-                                    b_pool + ((size_t)it.b_base * NT + (size_t)(cb >> 7) * it.KT + kt) * 3 * (size_t)TILE_BYTES;
-                                for (int p = 0; p < up; ++p) {
-                                    const int sl = (int)((vpos + (uint32_t)p) % C::NSLOT);
-                                    uint8_t *slot_base = smem + (size_t)sl * C::SLOT;
-                                    tc::mbar_expect_tx(&full[sl], (uint32_t)(TILE_BYTES + C::B_ROWS_BYTES));
-                                    tc::bulk_g2s(slot_base, ga + (size_t)p * TILE_BYTES, TILE_BYTES, &full[sl]);
-                                    tc::bulk_g2s(slot_base + TILE_BYTES, gb + (size_t)p * TILE_BYTES, TILE_BYTES, &full[sl]);
-                                }
-                            }
-                            vpos += (uint32_t)up;
-                            continue;
-                        }
                         const int s = g % C::STAGES;
                         const uint32_t round = g / C::STAGES;
                         if (!wait_x(&empty[s], (round & 1) ^ 1, abort_word)) {
@@ -609,14 +574,6 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                 }
             }
             // every stage this thread filled must have landed before the CTA may exit
-            if constexpr (VS) {
-                for (int sl = 0; sl < C::NSLOT; ++sl) {
-                    if ((uint32_t)sl >= vpos) continue;
-                    const uint32_t uses = (vpos - (uint32_t)sl + C::NSLOT - 1) / C::NSLOT;
-                    volatile int never = 0;
-                    tc::mbar_wait(&full[sl], (uses - 1) & 1, &never, la.wait_cycles);
-                }
-            }
 #pragma unroll
             for (int s = 0; s < C::STAGES; ++s) {
                 if (!filled[s]) continue;
@@ -633,8 +590,6 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
             uint32_t g = 0;     // K-tile (stage) counter
             uint32_t ga = 0;    // accumulator-fill counter
             uint32_t slot = 0;  // ring counter
-            uint32_t vpos = 0;  // VS: slots consumed so far (the producer's allocation order)
-            const uint32_t smem_base = tc::smem_u32(smem);
             bool any = false, stop = false;
             while (!stop) {
                 int ktiles = 0, up = P;
@@ -646,53 +601,6 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                 const int nprod = up == 2 ? 3 : 6;
                 const int kc = unit_kchain(up);
                 for (int i = 0; i < ktiles; ++i, ++g) {
-                    if constexpr (VS) {
-                        const int b = ga % C::NACC;
-                        const uint32_t use = ga / C::NACC;
-                        const bool first = i % kc == 0;
-                        const bool last = i % kc == kc - 1 || i == ktiles - 1;
-                        bool ok = !first || wait_x(&acce[b], (use & 1) ^ 1, abort_word);
-                        for (int p = 0; p < up && ok; ++p) {
-                            const uint32_t q = vpos + (uint32_t)p;
-                            ok = tc::mbar_wait(&full[q % C::NSLOT], (q / C::NSLOT) & 1, abort_word, la.wait_cycles);
-                        }
-                        if (!ok) {
-                            raise_abort();
-                            stop = true;
-                            break;
-                        }
-                        tc::fence_after_sync();
-                        const uint32_t dst = tmem + (uint32_t)(b * BN);
-                        uint32_t accum = first ? 0u : 1u;
-                        // descriptors of the tile's parts, once per tile (the issuing thread's
-                        // work per MMA must stay well under an MMA's duration)
-                        uint64_t dA[3], dB[3];
-#pragma unroll
-                        for (int p = 0; p < 3; ++p) {
-                            const uint32_t sl = (vpos + (uint32_t)p) % C::NSLOT;
-                            const uint32_t base = smem_base + sl * (uint32_t)C::SLOT;
-                            dA[p] = tc::smem_desc_sw128(base);
-                            dB[p] = tc::smem_desc_sw128(base + TILE_BYTES);
-                        }
-#pragma unroll
-                        for (int ks = 0; ks < 4; ++ks) {
-#pragma unroll
-                            for (int j = 0; j < 6; ++j) {
-                                if (j >= nprod) break;
-                                tc::mma_bf16(dst, dA[PA[j]] + (uint64_t)(ks * 2), dB[PB[j]] + (uint64_t)(ks * 2), IDESC,
-                                             accum);
-                                accum = 1;
-                            }
-                        }
-                        for (int p = 0; p < up; ++p) tc::mma_commit(&empty[(vpos + (uint32_t)p) % C::NSLOT]);
-                        if (last) {
-                            tc::mma_commit(&accf[b]);
-                            ++ga;
-                        }
-                        vpos += (uint32_t)up;
-                        any = true;
-                        continue;
-                    }
                     const int s = g % C::STAGES;
                     const uint32_t round = g / C::STAGES;
                     const int b = ga % C::NACC;
@@ -1090,7 +998,7 @@ int sm_count()
     return g_sm_count[dev];
 }
 
-template <int P, int BN, int S, bool PAIR, bool ORD, bool VS = false>
+template <int P, int BN, int S, bool PAIR, bool ORD>
 cudaError_t configure_tc()
 {
     static bool done[128];
@@ -1099,7 +1007,7 @@ cudaError_t configure_tc()
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 128) return cudaErrorInvalidDevice;
     if (done[dev]) return cudaSuccess;
-    e = cudaFuncSetAttribute(tc_gemm_kernel<P, BN, S, PAIR, ORD, VS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(tc_gemm_kernel<P, BN, S, PAIR, ORD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              TcCfg<P, BN, S, PAIR>::SMEM);
     if (e == cudaSuccess) done[dev] = true;
     return e;
@@ -1132,18 +1040,6 @@ cudaError_t launch_tc_cfg(const LaunchArgs &a, cudaStream_t s)
         cfg.numAttrs = 1;
         return cudaLaunchKernelEx(&cfg, tc_gemm_kernel<P, BN, S, true, ORD>, a);
     }
-}
-
-// The one-launch kernel: 3-part capacity, 128 columns, a ring of six 32-KiB slots.
-cudaError_t launch_tc_slots(const LaunchArgs &a, cudaStream_t s)
-{
-    using C = TcCfg<3, 128, 2, false>;
-    if (a.nunits <= 0) return cudaSuccess;
-    cudaError_t e = configure_tc<3, 128, 2, false, false, true>();
-    if (e != cudaSuccess) return e;
-    const int grid = std::min(a.nunits, sm_count());
-    tc_gemm_kernel<3, 128, 2, false, false, true><<<grid, C::THREADS, C::SMEM, s>>>(a);
-    return cudaGetLastError();
 }
 
 // Column-tile widths per product count; pipeline depth fills ~192-216 KiB of shared memory.
@@ -1580,7 +1476,6 @@ int Batch::units_for(Entry &e, const std::vector<int> &bn, cudaStream_t stream)
 
 namespace {
 int kchain_for(int P);
-bool slots_enabled();
 bool prefetch_enabled();
 }
 
@@ -1622,9 +1517,7 @@ int Batch::enqueue(Entry &e, cudaStream_t stream, int debug_flags, long long wai
         a.stall_level = (debug_flags & MXB_DEBUG_STALL_LEVEL) != 0;
         a.level_ns = level_ns;
         a.prefetch = prefetch_enabled();
-        // 128 columns: the slot-ring kernel (bf16x3 units hold two slots, bf16x6 units three)
-        const cudaError_t err = w == 128 && slots_enabled() ? launch_tc_slots(a, stream)
-                                                            : launch_tc(3, w, false, false, a, stream);
+        const cudaError_t err = launch_tc(3, w, false, false, a, stream);
         if (err != cudaSuccess) return batch_fail(std::string("one-launch evaluation: ") + cudaGetErrorString(err), MXB_ERR_CUDA);
         return MXB_OK;
     }
@@ -1752,13 +1645,6 @@ bool pairs_enabled()
 bool prefetch_enabled()
 {
     const char *e = getenv("MXB_TC_PREFETCH");
-    return !(e && *e == '0');
-}
-
-// MXB_TC_SLOTS=0 runs the one-launch mode with fixed stages (read when a graph is built).
-bool slots_enabled()
-{
-    const char *e = getenv("MXB_TC_SLOTS");
     return !(e && *e == '0');
 }
 
