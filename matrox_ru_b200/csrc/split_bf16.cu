@@ -156,7 +156,6 @@ struct LaunchArgs {
     int nlevels;            // chained levels (1: none); a unit's level is in TcUnit::chain
     int *level_done;        // per level: epilogue warps done with a unit of it (zero at launch)
     int stall_level;        // test hook: level 0 never reports done, so level 1's waits run out
-    int prefetch;           // the producer prefetches the next item's tiles into L2
     // profiling of chained launches (null otherwise): [0] the earliest CTA start, [1 + j] the
     // time the last unit of level j was written (%globaltimer, ns)
     unsigned long long *level_ns;
@@ -512,22 +511,6 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                     const TcItem it = ti[q];
                     const uint8_t *a_pool = pa->pool[it.a_pool];
                     const uint8_t *b_pool = pa->buf[it.b_buf];
-                    if (q + 1 < t.nitem && la.prefetch) {
-                        // ask L2 for the next item's operand tiles while this item streams through
-                        // the stages: one item of lead on the DRAM latency
-                        const TcItem nx = ti[q + 1];
-                        const uint8_t *na = pa->pool[nx.a_pool] + nx.a_off;
-                        const uint8_t *nb = pa->buf[nx.b_buf];
-                        for (int kt = 0; kt < nx.KT; ++kt) {
-                            if (a_ok)
-                                tc::bulk_prefetch_l2(na + ((size_t)mt * nx.KT + kt) * (size_t)up * TILE_BYTES,
-                                                     (uint32_t)up * TILE_BYTES);
-                            for (int hh = 0; hh < (C::B_ROWS + 127) / 128; ++hh)
-                                tc::bulk_prefetch_l2(nb + ((size_t)nx.b_base * NT + ((size_t)(cb >> 7) + hh) * nx.KT + kt) *
-                                                              3 * (size_t)TILE_BYTES,
-                                                     (uint32_t)up * TILE_BYTES);
-                        }
-                    }
                     for (int kt = 0; kt < it.KT; ++kt, ++g) {
                         const int s = g % C::STAGES;
                         const uint32_t round = g / C::STAGES;
@@ -1476,7 +1459,6 @@ int Batch::units_for(Entry &e, const std::vector<int> &bn, cudaStream_t stream)
 
 namespace {
 int kchain_for(int P);
-bool prefetch_enabled();
 }
 
 
@@ -1516,7 +1498,6 @@ int Batch::enqueue(Entry &e, cudaStream_t stream, int debug_flags, long long wai
         a.level_done = dLevel;
         a.stall_level = (debug_flags & MXB_DEBUG_STALL_LEVEL) != 0;
         a.level_ns = level_ns;
-        a.prefetch = prefetch_enabled();
         const cudaError_t err = launch_tc(3, w, false, false, a, stream);
         if (err != cudaSuccess) return batch_fail(std::string("one-launch evaluation: ") + cudaGetErrorString(err), MXB_ERR_CUDA);
         return MXB_OK;
@@ -1556,8 +1537,7 @@ int Batch::enqueue(Entry &e, cudaStream_t stream, int debug_flags, long long wai
                 a.nlevels = (int)(end - k);
                 a.level_done = dLevel + k;
                 a.stall_level = (debug_flags & MXB_DEBUG_STALL_LEVEL) != 0;
-                a.prefetch = prefetch_enabled();
-                int total = 0;
+                        int total = 0;
                 for (size_t j = k; j < end; ++j) total += e.unit_count[j];
                 a.nunits = total;
                 err = launch_tc(m.P, tile_width(bn[k]), tile_pair(bn[k]), writes_y && !e.order.empty(), a, stream);
@@ -1640,13 +1620,6 @@ bool pairs_enabled()
 }
 
 // MXB_TC_CHAIN=0 keeps every tree level in a launch of its own.
-// MXB_TC_PREFETCH=0 turns off the producer's L2 prefetch of the next item (read when a graph
-// is built).
-bool prefetch_enabled()
-{
-    const char *e = getenv("MXB_TC_PREFETCH");
-    return !(e && *e == '0');
-}
 
 // (read when an evaluation graph is built)
 bool chains_enabled()

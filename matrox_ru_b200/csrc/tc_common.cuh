@@ -107,12 +107,6 @@ __device__ __forceinline__ void acquire_counter(const int *ctr)
     (void)v;
 }
 
-// Bulk prefetch of global memory into L2 (a hint; `bytes` a multiple of 16).
-__device__ __forceinline__ void bulk_prefetch_l2(const void *src, uint32_t bytes)
-{
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(src), "r"(bytes) : "memory");
-}
-
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
 {
     asm volatile(
