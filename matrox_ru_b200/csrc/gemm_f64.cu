@@ -100,8 +100,10 @@ __global__ void __launch_bounds__(THREADS, 4)
 gemm_f64_kernel(const Task *__restrict__ tasks, const Item *__restrict__ items, Operands ops)
 {
     extern __shared__ __align__(16) double smem[];
-    const Task t = tasks[blockIdx.x];
-    const int n0 = blockIdx.y * BN;
+    // column tiles of one task run in neighbouring CTAs, so its A tiles come from DRAM once
+    const int ncol = (ops.nrhs + BN - 1) / BN;
+    const Task t = tasks[blockIdx.x / ncol];
+    const int n0 = (blockIdx.x % ncol) * BN;
     const int nrhs = ops.nrhs;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wm = warp & 1, wn = warp >> 1;
@@ -270,8 +272,9 @@ cudaError_t launch_gemm_f64(const Task *tasks, const Item *items, int ntasks, co
         configured[dev] = true;
     }
     if (ntasks <= 0) return cudaSuccess;
-    dim3 grid(ntasks, (ops.nrhs + BN - 1) / BN);
-    gemm_f64_kernel<<<grid, THREADS, SMEM_BYTES, stream>>>(tasks, items, ops);
+    const int64_t blocks = (int64_t)ntasks * ((ops.nrhs + BN - 1) / BN);
+    if (blocks > 0x7FFFFFFF) return cudaErrorInvalidConfiguration;
+    gemm_f64_kernel<<<(unsigned)blocks, THREADS, SMEM_BYTES, stream>>>(tasks, items, ops);
     return cudaGetLastError();
 }
 

@@ -255,7 +255,19 @@ void Plan::build_tasks(int tile)
     };
     auto end_launch = [&](std::vector<Launch> &L) {
         L.back().ntasks = (int)tasks.size() - L.back().task0;
-        if (L.back().ntasks == 0) L.pop_back();
+        if (L.back().ntasks == 0) {
+            L.pop_back();
+            return;
+        }
+        // longest tasks first: the CTAs of a launch start in task order, so the last wave holds
+        // the shortest tasks (each task owns its output tile, so the order changes no result)
+        auto cost = [&](const Task &t) {
+            int64_t k = 0;
+            for (int q = t.item0; q < t.item0 + t.nitem; ++q) k += items[q].K;
+            return k;
+        };
+        std::stable_sort(tasks.begin() + L.back().task0, tasks.end(),
+                         [&](const Task &a, const Task &b) { return cost(a) > cost(b); });
     };
     // per-node far lists (forward: pairs (c, y) for output c; adjoint: pairs (x, c))
     std::vector<std::vector<int>> far_out(numnodes), far_in(numnodes);

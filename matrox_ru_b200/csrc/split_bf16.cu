@@ -30,9 +30,12 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <memory>
+#include <queue>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "matrox_b200.h"
@@ -100,7 +103,14 @@ struct TcUnit {
     int32_t ktiles;  // K tiles of the task (sum over its items)
     int32_t chain;   // chained launches: parts << 28 | level << 20 | units of the level before
                      // (parts 2 or 3: the unit's operand parts when they differ from the launch's)
+    // Dataflow launches (LaunchArgs::deps): the unit loads its B tiles once the node counters
+    // dep0 / dep1 (-1: none) have counted need0 / need1 finished units (need0 | need1 << 16),
+    // and counts itself into counter `sig` (-1: none) once its output is written.
+    int32_t dep0, dep1;
+    int32_t need;
+    int32_t sig;
 };
+static_assert(sizeof(TcUnit) == 32, "TcUnit layout");
 
 struct SplitJob {     // one leaf block of W -> B-operand tiles
     int64_t src_row;  // leaf index
@@ -159,6 +169,9 @@ struct LaunchArgs {
     // profiling of chained launches (null otherwise): [0] the earliest CTA start, [1 + j] the
     // time the last unit of level j was written (%globaltimer, ns)
     unsigned long long *level_ns;
+    // dataflow launches (null otherwise): per-node completion counters, zero at launch; units
+    // wait for the nodes whose tiles they read instead of for whole levels (TcUnit::dep0/dep1)
+    int *deps;
 };
 
 // ---------------------------------------------------------------------------------------
@@ -295,16 +308,29 @@ __device__ __forceinline__ void transpose8(float (&x)[8], int lane)
 // tcgen05.mma.cta_group::2; each CTA stages its own 128 rows of A and half of the BN rows of
 // B, so a pair moves a third less operand data per flop than two single CTAs and has room for
 // a deeper pipeline.
+//
+// P = 4 ("dual", one-launch evaluations of mixed product counts, single CTAs only): the stage
+// memory serves two geometries in turn, STAGES 3-part stages for the units of bf16x6 products
+// and S2 2-part stages for those of bf16x3 products, so bf16x3 units keep a deeper pipeline
+// than 3-part stages would give them.  Each geometry has its own barriers and K-tile counter;
+// before the producer fills one geometry it waits until the MMAs are done with every stage of
+// the other.
 template <int P, int BN, int STAGES_, bool PAIR = false>
 struct TcCfg {
+    static constexpr bool DUAL = P == 4;
+    static constexpr int PP = DUAL ? 3 : P;                // parts of the (first) stage geometry
     static constexpr int STAGES = STAGES_;
     static constexpr int B_ROWS = PAIR ? BN / 2 : BN;      // B rows (output columns) staged per CTA
     static constexpr int B_ROWS_BYTES = B_ROWS * 128;      // one part of the staged B operand
-    static constexpr int A_BYTES = P * TILE_BYTES;
-    static constexpr int B_BYTES = P * B_ROWS_BYTES;
+    static constexpr int A_BYTES = PP * TILE_BYTES;
+    static constexpr int B_BYTES = PP * B_ROWS_BYTES;
     static constexpr int STAGE = A_BYTES + B_BYTES;
+    static constexpr int A2_BYTES = 2 * TILE_BYTES;        // second geometry (DUAL): 2 parts
+    static constexpr int STAGE2 = A2_BYTES + 2 * B_ROWS_BYTES;
+    static constexpr int S2 = DUAL ? (STAGES * STAGE) / STAGE2 : 0;
+    static constexpr int NBAR = STAGES + S2;               // full / empty / pair barriers
     static constexpr int SMEM = STAGES * STAGE + 1024 + 1024;  // + alignment, barriers, unit ring
-    static constexpr int NPROD = P == 2 ? 3 : 6;
+    static constexpr int NPROD = PP == 2 ? 3 : 6;
     static constexpr int EPI_WARPS = 8;          // two per TMEM lane quarter, one per column half
     static constexpr int RING = 16;              // work units published ahead of the readers
     // readers of a ring slot: MMA issuer and epilogue warps (+ the odd CTA's producer, relay
@@ -322,6 +348,7 @@ struct TcCfg {
     static constexpr int M_MMA = PAIR ? 256 : 128;
     static_assert(SMEM <= 232448, "shared memory");
     static_assert(B_ROWS % 64 == 0, "B rows per CTA");
+    static_assert(!DUAL || (!PAIR && S2 >= 1 && S2 <= 8 && STAGE2 % 1024 == 0), "dual stage geometry");
 };
 
 // Tensor-core FP32 accumulation is not round-to-nearest: its error grows with the number of
@@ -346,7 +373,7 @@ template <int P, int BN, int STAGES_, bool PAIR, bool ORD>
 __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_gemm_kernel(LaunchArgs la)
 {
     using C = TcCfg<P, BN, STAGES_, PAIR>;
-    constexpr int NB = C::STAGES;  // full / empty / pair barriers: one per stage
+    constexpr int NB = C::NBAR;  // full / empty / pair barriers: one per stage (of both geometries)
     constexpr int RING = C::RING;
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -441,11 +468,13 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
         if (lane == 0) {
             // ---------------- producer ----------------
             uint32_t g = 0;               // K-tile counter of this CTA
+            uint32_t g2 = 0;              // DUAL: K-tile counter of the 2-part geometry
+            bool geo2 = false;            // DUAL: the 2-part geometry holds the stage memory
             uint32_t slot = 0;            // ring counter
             int waited = 0;               // last chained level waited for
-            uint32_t filled[C::STAGES];   // rounds filled per stage (drained before exit)
+            uint32_t filled[C::NBAR];     // rounds filled per stage (drained before exit)
 #pragma unroll
-            for (int s = 0; s < C::STAGES; ++s) filled[s] = 0;
+            for (int s = 0; s < C::NBAR; ++s) filled[s] = 0;
             bool stop = false;
             while (!stop && !*abort_word) {
                 int u, kt_unit = 0;
@@ -496,6 +525,19 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                         waited = lvl;
                     }
                 }
+                if (la.deps) {
+                    // dataflow: the nodes whose tiles this unit reads have written them for this
+                    // column tile (every one of their units, every epilogue warp)
+                    bool ok = un.dep0 < 0 || tc::wait_counter(la.deps + un.dep0, (un.need & 0xFFFF) * C::UNIT_WRITERS,
+                                                              abort_word, la.wait_cycles);
+                    if (ok && un.dep1 >= 0)
+                        ok = tc::wait_counter(la.deps + un.dep1, (un.need >> 16) * C::UNIT_WRITERS, abort_word,
+                                              la.wait_cycles);
+                    if (!ok) {
+                        raise_abort();
+                        break;
+                    }
+                }
                 const TcTask t = la.tasks[un.task];
                 const PlanArgs *pa = la.plans + t.plan;
                 const int NT = pa->NT;
@@ -507,21 +549,35 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                 const bool a_ok = !PAIR || issuer || t.m0 + 128 < t.M;
                 const int up = unit_parts(un.chain);
                 const uint32_t tx = (a_ok ? (uint32_t)up * TILE_BYTES : 0u) + (uint32_t)up * C::B_ROWS_BYTES;
+                const bool two = C::DUAL && up == 2;  // DUAL: this unit fills the 2-part stages
+                if (C::DUAL && two != geo2 && t.nitem > 0) {
+                    // the other geometry's stages share this memory: wait until the MMAs are
+                    // done with every one of them
+                    const int s0 = geo2 ? C::STAGES : 0, s1 = geo2 ? C::NBAR : C::STAGES;
+                    for (int s = s0; s < s1 && !stop; ++s)
+                        if (filled[s] && !wait_x(&empty[s], (filled[s] - 1) & 1, abort_word)) {
+                            raise_abort();
+                            stop = true;
+                        }
+                    geo2 = two;
+                }
                 for (int q = 0; q < t.nitem && !stop; ++q) {
                     const TcItem it = ti[q];
                     const uint8_t *a_pool = pa->pool[it.a_pool];
                     const uint8_t *b_pool = pa->buf[it.b_buf];
-                    for (int kt = 0; kt < it.KT; ++kt, ++g) {
-                        const int s = g % C::STAGES;
-                        const uint32_t round = g / C::STAGES;
+                    for (int kt = 0; kt < it.KT; ++kt) {
+                        const uint32_t gc = two ? g2++ : g++;
+                        const int ns = two ? C::S2 : C::STAGES;
+                        const int s = (two ? C::STAGES : 0) + (int)(gc % ns);  // barrier / filled index
+                        const uint32_t round = gc / ns;
                         if (!wait_x(&empty[s], (round & 1) ^ 1, abort_word)) {
                             raise_abort();
                             stop = true;
                             break;
                         }
-                        if (la.stall_test && blockIdx.x == 0 && g == 0) continue;  // never filled
-                        uint8_t *sa = smem + s * C::STAGE;
-                        uint8_t *sb = sa + C::A_BYTES;
+                        if (la.stall_test && blockIdx.x == 0 && !two && gc == 0) continue;  // never filled
+                        uint8_t *sa = two ? smem + (s - C::STAGES) * C::STAGE2 : smem + s * C::STAGE;
+                        uint8_t *sb = sa + (two ? C::A2_BYTES : C::A_BYTES);
                         tc::mbar_expect_tx(&full[s], tx);
                         if (a_ok) {
                             const uint8_t *ga = a_pool + it.a_off + ((size_t)mt * it.KT + kt) * (size_t)up * TILE_BYTES;
@@ -534,7 +590,7 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                                 const uint8_t *gb =
                                     b_pool + ((size_t)it.b_base * NT + nt * it.KT + kt) * 3 * (size_t)TILE_BYTES;
 #pragma unroll
-                                for (int p = 0; p < P; ++p)
+                                for (int p = 0; p < C::PP; ++p)
                                     if (p < up)
                                         tc::bulk_g2s(sb + p * C::B_ROWS_BYTES + hh * TILE_BYTES,
                                                      gb + (size_t)p * TILE_BYTES, TILE_BYTES, &full[s]);
@@ -547,7 +603,7 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                                                     (size_t)TILE_BYTES +
                                                 (size_t)(cb & 127) * 128;
 #pragma unroll
-                            for (int p = 0; p < P; ++p)
+                            for (int p = 0; p < C::PP; ++p)
                                 if (p < up)
                                     tc::bulk_g2s(sb + p * C::B_ROWS_BYTES, gb + (size_t)p * TILE_BYTES, C::B_ROWS_BYTES,
                                                  &full[s]);
@@ -558,7 +614,7 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
             }
             // every stage this thread filled must have landed before the CTA may exit
 #pragma unroll
-            for (int s = 0; s < C::STAGES; ++s) {
+            for (int s = 0; s < C::NBAR; ++s) {
                 if (!filled[s]) continue;
                 volatile int never = 0;
                 tc::mbar_wait(&full[s], (filled[s] - 1) & 1, &never, la.wait_cycles);
@@ -571,6 +627,7 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
             constexpr int PA[6] = {0, 0, 1, 0, 1, 2};
             constexpr int PB[6] = {0, 1, 0, 2, 1, 0};
             uint32_t g = 0;     // K-tile (stage) counter
+            uint32_t g2 = 0;    // DUAL: K-tile counter of the 2-part geometry
             uint32_t ga = 0;    // accumulator-fill counter
             uint32_t slot = 0;  // ring counter
             bool any = false, stop = false;
@@ -583,9 +640,12 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                 }
                 const int nprod = up == 2 ? 3 : 6;
                 const int kc = unit_kchain(up);
-                for (int i = 0; i < ktiles; ++i, ++g) {
-                    const int s = g % C::STAGES;
-                    const uint32_t round = g / C::STAGES;
+                const bool two = C::DUAL && up == 2;
+                for (int i = 0; i < ktiles; ++i) {
+                    const uint32_t gc = two ? g2++ : g++;
+                    const int ns = two ? C::S2 : C::STAGES;
+                    const int s = (two ? C::STAGES : 0) + (int)(gc % ns);
+                    const uint32_t round = gc / ns;
                     const int b = ga % C::NACC;
                     const uint32_t use = ga / C::NACC;
                     const bool first = i % kc == 0;
@@ -600,8 +660,10 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                     tc::fence_after_sync();
                     // descriptors of the stage's part tiles; a byte offset o within the stage adds
                     // o >> 4 to the start-address field (shared addresses stay below 2^18)
-                    const uint32_t sa = tc::smem_u32(smem + s * C::STAGE);
-                    const uint64_t da = tc::smem_desc_sw128(sa), db = tc::smem_desc_sw128(sa + C::A_BYTES);
+                    const uint32_t sa =
+                        tc::smem_u32(two ? smem + (s - C::STAGES) * C::STAGE2 : smem + s * C::STAGE);
+                    const uint64_t da = tc::smem_desc_sw128(sa),
+                                   db = tc::smem_desc_sw128(sa + (two ? C::A2_BYTES : C::A_BYTES));
                     const uint32_t dst = tmem + (uint32_t)(b * BN);
                     uint32_t accum = first ? 0u : 1u;
 #pragma unroll
@@ -950,6 +1012,14 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                 }
             }
             if (la.nlevels > 1) ++pend;  // counted when the warp moves past this level
+            if (la.deps && un.sig >= 0) {
+                // dataflow: this warp's part of the unit is written; count it for the units
+                // that read it (the test hook keeps the units without inputs from counting)
+                asm volatile("fence.proxy.async.global;\n" ::: "memory");
+                __threadfence();
+                __syncwarp();
+                if (lane == 0 && !(la.stall_level && un.dep0 < 0)) atomicAdd(la.deps + un.sig, 1);
+            }
         }
     }
     __syncwarp();
@@ -1030,6 +1100,13 @@ cudaError_t launch_tc_cfg(const LaunchArgs &a, cudaStream_t s)
 template <bool ORD>
 cudaError_t launch_tc_ord(int P, int BN, bool pair, const LaunchArgs &a, cudaStream_t s)
 {
+    if (P == 4) {  // dual stage geometry (one-launch evaluations, leaf-blocked, single CTAs)
+        if constexpr (ORD) return cudaErrorNotSupported;
+        else {
+            if (pair) return cudaErrorNotSupported;
+            return BN == 128 ? launch_tc_cfg<4, 128, 2, false, false>(a, s) : launch_tc_cfg<4, 64, 3, false, false>(a, s);
+        }
+    }
     if (pair) {
         if (P == 2)
             return BN == 256 ? launch_tc_cfg<2, 256, 3, true, ORD>(a, s) : launch_tc_cfg<2, 128, 4, true, ORD>(a, s);
@@ -1069,6 +1146,8 @@ cudaError_t configure_all_tc_ord()
 cudaError_t configure_all_tc()
 {
     cudaError_t e = configure_all_tc_ord<false>();
+    if (e == cudaSuccess) e = configure_tc<4, 128, 2, false, false>();
+    if (e == cudaSuccess) e = configure_tc<4, 64, 3, false, false>();
     return e == cudaSuccess ? configure_all_tc_ord<true>() : e;
 }
 
@@ -1171,6 +1250,11 @@ struct Batch : public mxb_batch {
         PlanArgs *dPlans = nullptr;
         TcUnit *dUnits = nullptr;
         std::vector<int> unit_first, unit_count;
+        // dataflow launches: per op, whether its chained launch waits on node counters (the
+        // counters of every such launch in one array, zeroed before each evaluation)
+        std::vector<char> dataflow;
+        int *dDeps = nullptr;
+        int ndeps = 0;
         cudaGraphExec_t exec = nullptr;
     };
     std::vector<Entry> entries;
@@ -1189,9 +1273,12 @@ struct Batch : public mxb_batch {
         if (e.exec) cudaGraphExecDestroy(e.exec);
         if (e.dPlans) cudaFree(e.dPlans);
         if (e.dUnits) cudaFree(e.dUnits);
+        if (e.dDeps) cudaFree(e.dDeps);
         e.exec = nullptr;
         e.dPlans = nullptr;
         e.dUnits = nullptr;
+        e.dDeps = nullptr;
+        e.ndeps = 0;
     }
     void clear()
     {
@@ -1204,6 +1291,8 @@ struct Batch : public mxb_batch {
     int enqueue(Entry &e, cudaStream_t stream, int debug_flags, long long wait_cycles, const std::vector<int> &bn,
                 int only_op = -1);
     int units_for(Entry &e, const std::vector<int> &bn, cudaStream_t stream);
+    int dataflow_units(const Entry &e, size_t k, size_t end, const std::vector<int> &bn, std::vector<TcUnit> &units,
+                       int &ndeps) const;
     void chain_all(std::vector<int> &bn) const;
     int tune(Entry &e, std::vector<PlanArgs> pa, std::vector<int> &bn, cudaStream_t stream, long long wait_cycles);
     int tune_one_launch(Entry &e, std::vector<PlanArgs> pa, std::vector<int> &bn, cudaStream_t stream,
@@ -1346,6 +1435,197 @@ int64_t unit_group_bytes()
     return v;
 }
 
+// MXB_TC_DATAFLOW=0 keeps chained launches on level barriers (read when an evaluation graph is
+// built).
+bool dataflow_enabled()
+{
+    const char *e = getenv("MXB_TC_DATAFLOW");
+    return !(e && *e == '0');
+}
+
+// Dataflow schedule of a chained run of sweep ops [k, end): the up-sweep heights, or the
+// down-sweep depths with leaf down.  A node (the tasks of one output block: its row tiles)
+// depends on the nodes of earlier levels of the run whose output tiles its items read, and
+// each of its units waits, for its own column tile only, until those nodes' units have written
+// them -- instead of waiting for the whole level before.  The dependencies of a sweep form a
+// tree: up-sweep nodes read their two children, down-sweep nodes (and leaf down) their parent.
+//
+// The unit order comes from a list-scheduling simulation of the launch (one worker per CTA or
+// CTA pair, time in K tiles): whenever a worker claims, the next node is the
+// ready one (inputs finished in the simulation) that comes first in a depth-first order of the
+// tree -- post-order for the up sweep, pre-order for the down sweep -- with all its units
+// (column tile by column tile).  So a parent runs soon after its children while their tiles
+// are still in L2, a node's column tiles run together (its A tiles are read from DRAM once),
+// and the short top levels of one subtree overlap the wide lower levels of the next.  Every
+// unit's inputs come earlier in the list, and units are claimed in list order, so the waits
+// always end.
+//
+// Appends the run's units and returns 1; returns 0 (nothing appended) where the dependencies
+// are not a tree or a node reads tiles that its own or a later level writes, and the run then
+// keeps its level barriers.  Counters are allocated from `ndeps` on.
+int Batch::dataflow_units(const Entry &e, size_t k, size_t end, const std::vector<int> &bn, std::vector<TcUnit> &units,
+                          int &ndeps) const
+{
+    const bool pair = tile_pair(bn[k]);
+    const int w = tile_width(bn[k]);
+    struct Node {
+        int plan = 0, level = 0;
+        int64_t key = 0;         // tile K base of the output (OUT_TILES) or leaf index (OUT_Y)
+        std::vector<int> tasks;  // tasks that carry units (row tiles; the even one of a pair)
+        std::vector<int> dep;    // nodes whose output tiles this node reads
+        std::vector<int> cons;   // nodes that read this node's output tiles
+        int ncol = 0, kt = 0, ctr = -1, order = 0, unplaced = 0;
+        double ready = 0, finish = 0;
+    };
+    std::vector<Node> nodes;
+    std::map<std::tuple<int, int, int64_t>, int> by_out;  // (plan, tile buffer or -1 for Y, key)
+    for (size_t q = k; q < end; ++q) {
+        const MOp &m = ops[q];
+        if (m.phase == PH_SPLITW) return 0;
+        for (int t = m.first; t < m.first + m.count; ++t) {
+            const TcTask &tk = tasks[t];
+            if (tk.out_kind != OUT_TILES && tk.out_kind != OUT_Y) return 0;
+            const auto id = std::make_tuple((int)tk.plan, tk.out_kind == OUT_TILES ? (int)tk.t_buf : -1,
+                                            tk.out_kind == OUT_TILES ? tk.out_kt : tk.c_row);
+            auto it = by_out.find(id);
+            int n;
+            if (it == by_out.end()) {
+                n = (int)nodes.size();
+                by_out[id] = n;
+                Node nd;
+                nd.plan = tk.plan;
+                nd.level = (int)q;
+                nd.key = std::get<2>(id);
+                nd.ncol = (int)ceil_div(e.nrhs[tk.plan], w);
+                nodes.push_back(nd);
+            } else {
+                n = it->second;
+                if (nodes[n].level != (int)q) return 0;  // one output written at two levels
+            }
+            if (pair && tk.m0 % 256) continue;  // the pair's odd CTA takes rows m0 + 128
+            nodes[n].tasks.push_back(t);
+        }
+    }
+    for (int n = 0; n < (int)nodes.size(); ++n) {
+        Node &nd = nodes[n];
+        if (nd.tasks.empty()) return 0;
+        const TcTask &t0 = tasks[nd.tasks[0]];
+        for (int q = t0.item0; q < t0.item0 + t0.nitem; ++q) nd.kt += items[q].KT;
+        for (int t : nd.tasks) {
+            const TcTask &tk = tasks[t];
+            for (int q = tk.item0; q < tk.item0 + tk.nitem; ++q) {
+                auto it = by_out.find(std::make_tuple(nd.plan, (int)items[q].b_buf, items[q].b_base));
+                if (it == by_out.end()) continue;  // written before this launch
+                const int wn = it->second;
+                if (nodes[wn].level >= nd.level) return 0;
+                if (std::find(nd.dep.begin(), nd.dep.end(), wn) == nd.dep.end()) nd.dep.push_back(wn);
+            }
+        }
+        if (nd.dep.size() > 2 || nd.tasks.size() > 0xFFFF) return 0;
+    }
+    for (int n = 0; n < (int)nodes.size(); ++n)
+        for (int wn : nodes[n].dep) nodes[wn].cons.push_back(n);
+    bool in_tree = true, out_tree = true;
+    for (const Node &nd : nodes) {
+        in_tree &= nd.cons.size() <= 1;
+        out_tree &= nd.dep.size() <= 1;
+    }
+    if (!in_tree && !out_tree) return 0;
+
+    // depth-first order: children before parents (up sweep), parents before children (down)
+    auto tree_less = [&](int a, int b) {
+        return std::tie(nodes[a].plan, nodes[a].level, nodes[a].key) < std::tie(nodes[b].plan, nodes[b].level, nodes[b].key);
+    };
+    int next = 0;
+    std::vector<int> roots;
+    for (int n = 0; n < (int)nodes.size(); ++n)
+        if (in_tree ? nodes[n].cons.empty() : nodes[n].dep.empty()) roots.push_back(n);
+    std::sort(roots.begin(), roots.end(), tree_less);
+    std::function<void(int)> visit = [&](int n) {
+        std::vector<int> ch = in_tree ? nodes[n].dep : nodes[n].cons;
+        std::sort(ch.begin(), ch.end(), tree_less);
+        if (!in_tree) nodes[n].order = next++;
+        for (int c : ch) visit(c);
+        if (in_tree) nodes[n].order = next++;
+    };
+    for (int r : roots) visit(r);
+    if (next != (int)nodes.size()) return 0;
+
+    for (Node &nd : nodes)
+        if (!nd.cons.empty()) {
+            nd.ctr = ndeps;
+            ndeps += nd.ncol;
+        }
+
+    // list scheduling (simulated, time in K tiles): one worker per CTA (pair), which claims its
+    // next unit once it has issued the last loads of the current one, i.e. about STAGES K
+    // tiles before the current unit's MMAs end -- a unit claimed before its inputs are written
+    // holds its CTA until they are
+    const int workers = std::max(1, pair ? sm_count() / 2 : sm_count());
+    struct Cta {
+        double claim, mma_free;
+        bool operator>(const Cta &o) const { return claim > o.claim; }
+    };
+    std::priority_queue<Cta, std::vector<Cta>, std::greater<Cta>> ctas;
+    for (int i = 0; i < workers; ++i) ctas.push(Cta{0.0, 0.0});
+    constexpr double STAGES_KT = 2.0;
+    auto later_order = [&](int a, int b) { return nodes[a].order > nodes[b].order; };
+    auto later_ready = [&](int a, int b) { return nodes[a].ready > nodes[b].ready; };
+    std::priority_queue<int, std::vector<int>, decltype(later_order)> ready(later_order);
+    std::priority_queue<int, std::vector<int>, decltype(later_ready)> waiting(later_ready);
+    for (int n = 0; n < (int)nodes.size(); ++n) {
+        nodes[n].unplaced = (int)nodes[n].dep.size();
+        if (!nodes[n].unplaced) waiting.push(n);
+    }
+    for (size_t placed = 0; placed < nodes.size(); ++placed) {
+        const double now = ctas.top().claim;
+        while (!waiting.empty() && nodes[waiting.top()].ready <= now) {
+            ready.push(waiting.top());
+            waiting.pop();
+        }
+        int g;
+        if (!ready.empty()) {
+            g = ready.top();
+            ready.pop();
+        } else if (!waiting.empty()) {
+            g = waiting.top();  // nothing ready: the node whose inputs finish first
+            waiting.pop();
+        } else {
+            return batch_fail("dataflow schedule: a node's inputs are never written");
+        }
+        Node &nd = nodes[g];
+        int need = 0;
+        for (size_t d = 0; d < nd.dep.size(); ++d) need |= (int)nodes[nd.dep[d]].tasks.size() << (16 * d);
+        for (int c = 0; c < nd.ncol; ++c)
+            for (int t : nd.tasks) {
+                Cta w = ctas.top();
+                ctas.pop();
+                const double load = std::max(w.claim, nd.ready);  // the producer waits for inputs
+                const double mma = std::max(load + 1.0, w.mma_free);
+                w.mma_free = mma + nd.kt;
+                w.claim = std::max(load, mma + std::max(0.0, nd.kt - STAGES_KT));
+                ctas.push(w);
+                nd.finish = std::max(nd.finish, mma + nd.kt + 1.0);
+                TcUnit u{};
+                u.task = t;
+                u.col = c;
+                u.ktiles = nd.kt;
+                u.chain = 0;
+                u.dep0 = nd.dep.size() > 0 ? nodes[nd.dep[0]].ctr + c : -1;
+                u.dep1 = nd.dep.size() > 1 ? nodes[nd.dep[1]].ctr + c : -1;
+                u.need = need;
+                u.sig = nd.ctr >= 0 ? nd.ctr + c : -1;
+                units.push_back(u);
+            }
+        for (int cn : nd.cons) {
+            Node &cd = nodes[cn];
+            cd.ready = std::max(cd.ready, nd.finish);
+            if (--cd.unplaced == 0) waiting.push(cn);
+        }
+    }
+    return 1;
+}
+
 // Work units of every TC op for this entry's nrhs and column-tile choices.
 // The list is uploaded on `stream`, ahead of the launches that read it.
 int Batch::units_for(Entry &e, const std::vector<int> &bn, cudaStream_t stream)
@@ -1381,10 +1661,28 @@ int Batch::units_for(Entry &e, const std::vector<int> &bn, cudaStream_t stream)
             e.unit_count[k] = (int)units.size() - e.unit_first[k];
         }
     }
+    e.dataflow.assign(ops.size(), 0);
+    int ndeps = 0;
     for (size_t k = 0; k < ops.size() && !one_launch; ++k) {
         const MOp &m = ops[k];
         e.unit_first[k] = (int)units.size();
         if (m.phase == PH_SPLITW) continue;
+        if (!(bn[k] & TILE_CHAIN) && dataflow_enabled()) {
+            // a chain head: its run waits on node counters where the sweep's dependencies allow
+            size_t end = k + 1;
+            while (end < ops.size() && ops[end].phase != PH_SPLITW && (bn[end] & TILE_CHAIN)) ++end;
+            if (end - k >= 2) {
+                const int r = dataflow_units(e, k, end, bn, units, ndeps);
+                if (r < 0) return r;
+                if (r == 1) {
+                    e.dataflow[k] = 1;
+                    e.unit_count[k] = (int)units.size() - e.unit_first[k];
+                    for (size_t q = k + 1; q < end; ++q) e.unit_first[q] = (int)units.size();
+                    k = end - 1;
+                    continue;
+                }
+            }
+        }
         const bool pair = tile_pair(bn[k]);
         // level of this op in its chained launch, and the units of the level before it
         int level = 0;
@@ -1450,6 +1748,13 @@ int Batch::units_for(Entry &e, const std::vector<int> &bn, cudaStream_t stream)
     }
     if (e.dUnits) cudaFree(e.dUnits);
     e.dUnits = nullptr;
+    if (e.dDeps) cudaFree(e.dDeps);
+    e.dDeps = nullptr;
+    e.ndeps = ndeps;
+    if (ndeps) {
+        const cudaError_t derr = cudaMalloc(&e.dDeps, (size_t)ndeps * sizeof(int));
+        if (derr != cudaSuccess) return batch_fail(std::string("node counters: ") + cudaGetErrorString(derr), MXB_ERR_NOMEM);
+    }
     cudaError_t err = cudaMalloc(&e.dUnits, std::max<size_t>(units.size(), 1) * sizeof(TcUnit));
     if (err == cudaSuccess && !units.empty())
         err = cudaMemcpyAsync(e.dUnits, units.data(), units.size() * sizeof(TcUnit), cudaMemcpyHostToDevice, stream);
@@ -1472,6 +1777,8 @@ int Batch::enqueue(Entry &e, cudaStream_t stream, int debug_flags, long long wai
     // one allocation: dLevel follows dNext)
     const size_t nops = std::max<size_t>(ops.size(), 1);
     cudaError_t zerr = cudaMemsetAsync(dNext, 0, 2 * nops * sizeof(int), stream);
+    if (zerr == cudaSuccess && e.ndeps && (only_op < 0 || (only_op < (int)e.dataflow.size() && e.dataflow[only_op])))
+        zerr = cudaMemsetAsync(e.dDeps, 0, (size_t)e.ndeps * sizeof(int), stream);
     if (zerr != cudaSuccess) return batch_fail(std::string("work-unit counters: ") + cudaGetErrorString(zerr), MXB_ERR_CUDA);
     if (one_launch) {
         // every op is a level of the launch of op 0 (profiling asks for op 0 to time it)
@@ -1498,7 +1805,10 @@ int Batch::enqueue(Entry &e, cudaStream_t stream, int debug_flags, long long wai
         a.level_done = dLevel;
         a.stall_level = (debug_flags & MXB_DEBUG_STALL_LEVEL) != 0;
         a.level_ns = level_ns;
-        const cudaError_t err = launch_tc(3, w, false, false, a, stream);
+        // dual stage geometry: the bf16x3 levels (couplings, near field) get 2-part stages
+        // (MXB_ONE_LAUNCH_DUAL=0: every level on 3-part stages)
+        const char *dv = getenv("MXB_ONE_LAUNCH_DUAL");
+        const cudaError_t err = launch_tc((dv && *dv == '0') ? 3 : 4, w, false, false, a, stream);
         if (err != cudaSuccess) return batch_fail(std::string("one-launch evaluation: ") + cudaGetErrorString(err), MXB_ERR_CUDA);
         return MXB_OK;
     }
@@ -1536,6 +1846,10 @@ int Batch::enqueue(Entry &e, cudaStream_t stream, int debug_flags, long long wai
                 if (end - k > (size_t)MAX_CHAIN) return batch_fail("a chained launch has too many levels");
                 a.nlevels = (int)(end - k);
                 a.level_done = dLevel + k;
+                if (k < e.dataflow.size() && e.dataflow[k]) {
+                    a.nlevels = 1;  // node counters instead of level barriers
+                    a.deps = e.dDeps;
+                }
                 a.stall_level = (debug_flags & MXB_DEBUG_STALL_LEVEL) != 0;
                         int total = 0;
                 for (size_t j = k; j < end; ++j) total += e.unit_count[j];
@@ -2041,6 +2355,15 @@ int Batch::profile(const double *const *W, double *const *Y, const int *nrhs, cu
         if (n && cudaMemcpy(units.data(), e->dUnits, n * sizeof(TcUnit), cudaMemcpyDeviceToHost) != cudaSuccess)
             rc = batch_fail("profile: reading the work units failed", MXB_ERR_CUDA);
     }
+    // the op of each unit, from its task (the units of a dataflow launch interleave its ops)
+    std::vector<int> task_op(tasks.size(), -1);
+    for (size_t k = 0; k < ops.size(); ++k) {
+        if (ops[k].phase == PH_SPLITW) {
+            for (int t = split_task0; t < split_task0 + split_tasks; ++t) task_op[t] = (int)k;
+            continue;
+        }
+        for (int t = ops[k].first; t < ops[k].first + ops[k].count; ++t) task_op[t] = (int)k;
+    }
     for (size_t k = 0; k < ops.size() && !rc && (int)k < cap && out; ++k) {
         const MOp &m = ops[k];
         mxb_op_profile &o = out[k];
@@ -2050,22 +2373,25 @@ int Batch::profile(const double *const *W, double *const *Y, const int *nrhs, cu
         o.width = tile_width(e->bn[k]);
         o.pair = tile_pair(e->bn[k]) ? 1 : 0;
         o.chained = one_launch ? (k > 0) : ((m.phase != PH_SPLITW && (e->bn[k] & TILE_CHAIN)) ? 1 : 0);
-        o.units = e->unit_count[k];
-        const double products = m.P == 2 ? 3.0 : 6.0;
-        const int tile_rows = o.pair ? 256 : 128;
-        for (int u = e->unit_first[k]; u < e->unit_first[k] + e->unit_count[k]; ++u) {
-            const TcTask &t = tasks[units[u].task];
-            const double rows = std::min(tile_rows, t.M - t.m0);
-            const double cols = std::min(o.width, nr[t.plan] - units[u].col * o.width);
-            for (int q = t.item0; q < t.item0 + t.nitem; ++q) {
-                o.flops += 2.0 * rows * items[q].K * cols;
-                o.issued_flops += products * 2.0 * tile_rows * (64.0 * items[q].KT) * o.width;
-            }
-        }
         cudaEventElapsedTime(&o.ms, ev[k], ev[k + 1]);
         if (o.chained) o.ms = 0.f;
         if (one_launch && lns[k + 1] >= lns[k] && lns[0] != ~0ull)
             o.level_ms = (float)((double)(lns[k + 1] - (k ? lns[k] : lns[0])) * 1e-6);
+    }
+    for (size_t u = 0; u < units.size() && !rc && out; ++u) {
+        const TcTask &t = tasks[units[u].task];
+        const int k = task_op[units[u].task];
+        if (k < 0 || k >= cap) continue;
+        mxb_op_profile &o = out[k];
+        ++o.units;
+        const double products = ops[k].P == 2 ? 3.0 : 6.0;
+        const int tile_rows = o.pair ? 256 : 128;
+        const double rows = std::min(tile_rows, t.M - t.m0);
+        const double cols = std::min(o.width, nr[t.plan] - units[u].col * o.width);
+        for (int q = t.item0; q < t.item0 + t.nitem; ++q) {
+            o.flops += 2.0 * rows * items[q].K * cols;
+            o.issued_flops += products * 2.0 * tile_rows * (64.0 * items[q].KT) * o.width;
+        }
     }
     for (cudaEvent_t x : ev)
         if (x) cudaEventDestroy(x);

@@ -45,11 +45,15 @@ def test_hooks_rejected_on_fp64_plans(torch, small_cases):
     assert e.value.code == _lib.MXB_ERR_UNSUPPORTED
 
 
-def test_chained_levels_match_separate_launches(torch, small_cases):
-    """Up-sweep heights (and down-sweep depths with leaf down) run as one launch each, levels
-    waiting for each other on the device: the same result as the separate launches (the
-    evaluation is exact in the chaining; only the tile schedule changes), and fewer launches."""
+@pytest.mark.parametrize("dataflow", ["1", "0"])
+def test_chained_levels_match_separate_launches(torch, small_cases, monkeypatch, dataflow):
+    """Up-sweep heights (and down-sweep depths with leaf down) run as one launch each, the
+    levels waiting for each other on the device -- node by node through per-node counters
+    (dataflow, the default) or level by level (MXB_TC_DATAFLOW=0): the same result as the
+    separate launches (the evaluation is exact in the chaining; only the tile schedule
+    changes), and fewer launches."""
     import os
+    monkeypatch.setenv("MXB_TC_DATAFLOW", dataflow)
     for name in ("h2b", "hss", "ragged"):
         cds = small_cases[name]
         r = 200
@@ -78,10 +82,12 @@ def test_chained_levels_match_separate_launches(torch, small_cases):
         assert all(x["ms"] == 0.0 for x in prof if x["chained"])
 
 
-def test_level_barrier_that_runs_out_reports_timeout(torch, small_cases):
-    """The first level of a chained launch never reports its units done (test hook): the
-    next level's bounded wait runs out, the plan reports MXB_ERR_TIMEOUT, and the same plan
-    then computes correctly."""
+@pytest.mark.parametrize("dataflow", ["1", "0"])
+def test_level_barrier_that_runs_out_reports_timeout(torch, small_cases, monkeypatch, dataflow):
+    """The first level of a chained launch (dataflow: the units without inputs in the launch)
+    never reports its units done (test hook): the next level's bounded wait runs out, the plan
+    reports MXB_ERR_TIMEOUT, and the same plan then computes correctly."""
+    monkeypatch.setenv("MXB_TC_DATAFLOW", dataflow)
     cds = small_cases["h2b"]
     r = 64
     TW = np.random.default_rng(4).standard_normal(cds.n * r)
