@@ -78,8 +78,10 @@ def batched_report(args, count=64, seed=20261204):
         h = float(rng.uniform(0.5, 3.0))
         r = int(np.exp(rng.uniform(np.log(32), np.log(512))))
         X = S.gaussian_mixture(n, d, 16, -2.0, 2.0, 0.3, 1.0, seed=seed + i)
+        # the per-node IDs of each tree level factored on the GPU (the same ranks and skeletons
+        # as the host ID), which keeps the 64 builds to about a minute
         cds = S.build_cds(X, S.KernelSpec(kind, h), leaf_size=256, budget=0.03, tol=1e-5, max_rank=256,
-                          seed=seed + i)
+                          seed=seed + i, id_on_gpu=True)
         g = torch.Generator(device=dev).manual_seed(seed + i)
         TW = torch.randn(cds.n * r, dtype=torch.float32, device=dev, generator=g).double()
         p64 = H.Plan(cds, "fp64")
@@ -134,6 +136,7 @@ def batched_report(args, count=64, seed=20261204):
     # each level's span inside the one launch (the kernel's own timer), and the level launches
     one_levels = [[x["phase"], x["level"], round(x["level_ms"], 4)] for x in one.profile(TWs, nrhs, outs1)]
     one.status()
+
     multi_launches = [[x["phase"], x["level"], x["width"], "chained" if x["chained"] else "launch", round(x["ms"], 4)]
                       for x in batch.profile(TWs, nrhs, outs)]
     batch.status()

@@ -308,29 +308,16 @@ __device__ __forceinline__ void transpose8(float (&x)[8], int lane)
 // tcgen05.mma.cta_group::2; each CTA stages its own 128 rows of A and half of the BN rows of
 // B, so a pair moves a third less operand data per flop than two single CTAs and has room for
 // a deeper pipeline.
-//
-// P = 4 ("dual", one-launch evaluations of mixed product counts, single CTAs only): the stage
-// memory serves two geometries in turn, STAGES 3-part stages for the units of bf16x6 products
-// and S2 2-part stages for those of bf16x3 products, so bf16x3 units keep a deeper pipeline
-// than 3-part stages would give them.  Each geometry has its own barriers and K-tile counter;
-// before the producer fills one geometry it waits until the MMAs are done with every stage of
-// the other.
 template <int P, int BN, int STAGES_, bool PAIR = false>
 struct TcCfg {
-    static constexpr bool DUAL = P == 4;
-    static constexpr int PP = DUAL ? 3 : P;                // parts of the (first) stage geometry
     static constexpr int STAGES = STAGES_;
     static constexpr int B_ROWS = PAIR ? BN / 2 : BN;      // B rows (output columns) staged per CTA
     static constexpr int B_ROWS_BYTES = B_ROWS * 128;      // one part of the staged B operand
-    static constexpr int A_BYTES = PP * TILE_BYTES;
-    static constexpr int B_BYTES = PP * B_ROWS_BYTES;
+    static constexpr int A_BYTES = P * TILE_BYTES;
+    static constexpr int B_BYTES = P * B_ROWS_BYTES;
     static constexpr int STAGE = A_BYTES + B_BYTES;
-    static constexpr int A2_BYTES = 2 * TILE_BYTES;        // second geometry (DUAL): 2 parts
-    static constexpr int STAGE2 = A2_BYTES + 2 * B_ROWS_BYTES;
-    static constexpr int S2 = DUAL ? (STAGES * STAGE) / STAGE2 : 0;
-    static constexpr int NBAR = STAGES + S2;               // full / empty / pair barriers
     static constexpr int SMEM = STAGES * STAGE + 1024 + 1024;  // + alignment, barriers, unit ring
-    static constexpr int NPROD = PP == 2 ? 3 : 6;
+    static constexpr int NPROD = P == 2 ? 3 : 6;
     static constexpr int EPI_WARPS = 8;          // two per TMEM lane quarter, one per column half
     static constexpr int RING = 16;              // work units published ahead of the readers
     // readers of a ring slot: MMA issuer and epilogue warps (+ the odd CTA's producer, relay
@@ -348,7 +335,6 @@ struct TcCfg {
     static constexpr int M_MMA = PAIR ? 256 : 128;
     static_assert(SMEM <= 232448, "shared memory");
     static_assert(B_ROWS % 64 == 0, "B rows per CTA");
-    static_assert(!DUAL || (!PAIR && S2 >= 1 && S2 <= 8 && STAGE2 % 1024 == 0), "dual stage geometry");
 };
 
 // Tensor-core FP32 accumulation is not round-to-nearest: its error grows with the number of
@@ -373,7 +359,7 @@ template <int P, int BN, int STAGES_, bool PAIR, bool ORD>
 __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_gemm_kernel(LaunchArgs la)
 {
     using C = TcCfg<P, BN, STAGES_, PAIR>;
-    constexpr int NB = C::NBAR;  // full / empty / pair barriers: one per stage (of both geometries)
+    constexpr int NB = C::STAGES;  // full / empty / pair barriers: one per stage
     constexpr int RING = C::RING;
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -468,13 +454,11 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
         if (lane == 0) {
             // ---------------- producer ----------------
             uint32_t g = 0;               // K-tile counter of this CTA
-            uint32_t g2 = 0;              // DUAL: K-tile counter of the 2-part geometry
-            bool geo2 = false;            // DUAL: the 2-part geometry holds the stage memory
             uint32_t slot = 0;            // ring counter
             int waited = 0;               // last chained level waited for
-            uint32_t filled[C::NBAR];     // rounds filled per stage (drained before exit)
+            uint32_t filled[C::STAGES];   // rounds filled per stage (drained before exit)
 #pragma unroll
-            for (int s = 0; s < C::NBAR; ++s) filled[s] = 0;
+            for (int s = 0; s < C::STAGES; ++s) filled[s] = 0;
             bool stop = false;
             while (!stop && !*abort_word) {
                 int u, kt_unit = 0;
@@ -549,35 +533,21 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                 const bool a_ok = !PAIR || issuer || t.m0 + 128 < t.M;
                 const int up = unit_parts(un.chain);
                 const uint32_t tx = (a_ok ? (uint32_t)up * TILE_BYTES : 0u) + (uint32_t)up * C::B_ROWS_BYTES;
-                const bool two = C::DUAL && up == 2;  // DUAL: this unit fills the 2-part stages
-                if (C::DUAL && two != geo2 && t.nitem > 0) {
-                    // the other geometry's stages share this memory: wait until the MMAs are
-                    // done with every one of them
-                    const int s0 = geo2 ? C::STAGES : 0, s1 = geo2 ? C::NBAR : C::STAGES;
-                    for (int s = s0; s < s1 && !stop; ++s)
-                        if (filled[s] && !wait_x(&empty[s], (filled[s] - 1) & 1, abort_word)) {
-                            raise_abort();
-                            stop = true;
-                        }
-                    geo2 = two;
-                }
                 for (int q = 0; q < t.nitem && !stop; ++q) {
                     const TcItem it = ti[q];
                     const uint8_t *a_pool = pa->pool[it.a_pool];
                     const uint8_t *b_pool = pa->buf[it.b_buf];
-                    for (int kt = 0; kt < it.KT; ++kt) {
-                        const uint32_t gc = two ? g2++ : g++;
-                        const int ns = two ? C::S2 : C::STAGES;
-                        const int s = (two ? C::STAGES : 0) + (int)(gc % ns);  // barrier / filled index
-                        const uint32_t round = gc / ns;
+                    for (int kt = 0; kt < it.KT; ++kt, ++g) {
+                        const int s = g % C::STAGES;
+                        const uint32_t round = g / C::STAGES;
                         if (!wait_x(&empty[s], (round & 1) ^ 1, abort_word)) {
                             raise_abort();
                             stop = true;
                             break;
                         }
-                        if (la.stall_test && blockIdx.x == 0 && !two && gc == 0) continue;  // never filled
-                        uint8_t *sa = two ? smem + (s - C::STAGES) * C::STAGE2 : smem + s * C::STAGE;
-                        uint8_t *sb = sa + (two ? C::A2_BYTES : C::A_BYTES);
+                        if (la.stall_test && blockIdx.x == 0 && g == 0) continue;  // never filled
+                        uint8_t *sa = smem + s * C::STAGE;
+                        uint8_t *sb = sa + C::A_BYTES;
                         tc::mbar_expect_tx(&full[s], tx);
                         if (a_ok) {
                             const uint8_t *ga = a_pool + it.a_off + ((size_t)mt * it.KT + kt) * (size_t)up * TILE_BYTES;
@@ -590,7 +560,7 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                                 const uint8_t *gb =
                                     b_pool + ((size_t)it.b_base * NT + nt * it.KT + kt) * 3 * (size_t)TILE_BYTES;
 #pragma unroll
-                                for (int p = 0; p < C::PP; ++p)
+                                for (int p = 0; p < P; ++p)
                                     if (p < up)
                                         tc::bulk_g2s(sb + p * C::B_ROWS_BYTES + hh * TILE_BYTES,
                                                      gb + (size_t)p * TILE_BYTES, TILE_BYTES, &full[s]);
@@ -603,7 +573,7 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                                                     (size_t)TILE_BYTES +
                                                 (size_t)(cb & 127) * 128;
 #pragma unroll
-                            for (int p = 0; p < C::PP; ++p)
+                            for (int p = 0; p < P; ++p)
                                 if (p < up)
                                     tc::bulk_g2s(sb + p * C::B_ROWS_BYTES, gb + (size_t)p * TILE_BYTES, C::B_ROWS_BYTES,
                                                  &full[s]);
@@ -614,7 +584,7 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
             }
             // every stage this thread filled must have landed before the CTA may exit
 #pragma unroll
-            for (int s = 0; s < C::NBAR; ++s) {
+            for (int s = 0; s < C::STAGES; ++s) {
                 if (!filled[s]) continue;
                 volatile int never = 0;
                 tc::mbar_wait(&full[s], (filled[s] - 1) & 1, &never, la.wait_cycles);
@@ -627,7 +597,6 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
             constexpr int PA[6] = {0, 0, 1, 0, 1, 2};
             constexpr int PB[6] = {0, 1, 0, 2, 1, 0};
             uint32_t g = 0;     // K-tile (stage) counter
-            uint32_t g2 = 0;    // DUAL: K-tile counter of the 2-part geometry
             uint32_t ga = 0;    // accumulator-fill counter
             uint32_t slot = 0;  // ring counter
             bool any = false, stop = false;
@@ -640,12 +609,9 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                 }
                 const int nprod = up == 2 ? 3 : 6;
                 const int kc = unit_kchain(up);
-                const bool two = C::DUAL && up == 2;
-                for (int i = 0; i < ktiles; ++i) {
-                    const uint32_t gc = two ? g2++ : g++;
-                    const int ns = two ? C::S2 : C::STAGES;
-                    const int s = (two ? C::STAGES : 0) + (int)(gc % ns);
-                    const uint32_t round = gc / ns;
+                for (int i = 0; i < ktiles; ++i, ++g) {
+                    const int s = g % C::STAGES;
+                    const uint32_t round = g / C::STAGES;
                     const int b = ga % C::NACC;
                     const uint32_t use = ga / C::NACC;
                     const bool first = i % kc == 0;
@@ -660,10 +626,8 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                     tc::fence_after_sync();
                     // descriptors of the stage's part tiles; a byte offset o within the stage adds
                     // o >> 4 to the start-address field (shared addresses stay below 2^18)
-                    const uint32_t sa =
-                        tc::smem_u32(two ? smem + (s - C::STAGES) * C::STAGE2 : smem + s * C::STAGE);
-                    const uint64_t da = tc::smem_desc_sw128(sa),
-                                   db = tc::smem_desc_sw128(sa + (two ? C::A2_BYTES : C::A_BYTES));
+                    const uint32_t sa = tc::smem_u32(smem + s * C::STAGE);
+                    const uint64_t da = tc::smem_desc_sw128(sa), db = tc::smem_desc_sw128(sa + C::A_BYTES);
                     const uint32_t dst = tmem + (uint32_t)(b * BN);
                     uint32_t accum = first ? 0u : 1u;
 #pragma unroll
@@ -1100,13 +1064,6 @@ cudaError_t launch_tc_cfg(const LaunchArgs &a, cudaStream_t s)
 template <bool ORD>
 cudaError_t launch_tc_ord(int P, int BN, bool pair, const LaunchArgs &a, cudaStream_t s)
 {
-    if (P == 4) {  // dual stage geometry (one-launch evaluations, leaf-blocked, single CTAs)
-        if constexpr (ORD) return cudaErrorNotSupported;
-        else {
-            if (pair) return cudaErrorNotSupported;
-            return BN == 128 ? launch_tc_cfg<4, 128, 2, false, false>(a, s) : launch_tc_cfg<4, 64, 3, false, false>(a, s);
-        }
-    }
     if (pair) {
         if (P == 2)
             return BN == 256 ? launch_tc_cfg<2, 256, 3, true, ORD>(a, s) : launch_tc_cfg<2, 128, 4, true, ORD>(a, s);
@@ -1146,8 +1103,6 @@ cudaError_t configure_all_tc_ord()
 cudaError_t configure_all_tc()
 {
     cudaError_t e = configure_all_tc_ord<false>();
-    if (e == cudaSuccess) e = configure_tc<4, 128, 2, false, false>();
-    if (e == cudaSuccess) e = configure_tc<4, 64, 3, false, false>();
     return e == cudaSuccess ? configure_all_tc_ord<true>() : e;
 }
 
@@ -1805,10 +1760,7 @@ int Batch::enqueue(Entry &e, cudaStream_t stream, int debug_flags, long long wai
         a.level_done = dLevel;
         a.stall_level = (debug_flags & MXB_DEBUG_STALL_LEVEL) != 0;
         a.level_ns = level_ns;
-        // dual stage geometry: the bf16x3 levels (couplings, near field) get 2-part stages
-        // (MXB_ONE_LAUNCH_DUAL=0: every level on 3-part stages)
-        const char *dv = getenv("MXB_ONE_LAUNCH_DUAL");
-        const cudaError_t err = launch_tc((dv && *dv == '0') ? 3 : 4, w, false, false, a, stream);
+        const cudaError_t err = launch_tc(3, w, false, false, a, stream);
         if (err != cudaSuccess) return batch_fail(std::string("one-launch evaluation: ") + cudaGetErrorString(err), MXB_ERR_CUDA);
         return MXB_OK;
     }

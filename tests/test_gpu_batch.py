@@ -150,14 +150,10 @@ def test_batch_mixes_split_modes(torch):
         assert np.linalg.norm(alone - o.cpu().numpy()) <= 1e-6 * np.linalg.norm(want), m
 
 
-@pytest.mark.parametrize("dual", ["1", "0"])
-def test_one_launch_batch(torch, monkeypatch, dual):
+def test_one_launch_batch(torch):
     """MXB_BATCH_ONE_LAUNCH: the W split and every level of every plan (mixed split modes
     included) run as ONE launch with device-side level barriers; the results match the oracle
-    and the level-launch evaluation of the same batch.  Both pipelines: the stage memory
-    switching between 3-part and 2-part stages (default) and 3-part stages for every level
-    (MXB_ONE_LAUNCH_DUAL=0)."""
-    monkeypatch.setenv("MXB_ONE_LAUNCH_DUAL", dual)
+    and the level-launch evaluation of the same batch."""
     cases = make_cases(5, seed=11)
     modes = ["split_bf16", "split_bf16_far6", "split_bf16", "split_bf16_x6", "split_bf16"]
     plans = [H.Plan(c, m) for (c, _), m in zip(cases, modes)]
