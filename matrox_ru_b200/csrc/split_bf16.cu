@@ -36,6 +36,7 @@
 #include <queue>
 #include <string>
 #include <tuple>
+#include <type_traits>
 #include <vector>
 
 #include "matrox_b200.h"
@@ -460,17 +461,41 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
 #pragma unroll
             for (int s = 0; s < C::STAGES; ++s) filled[s] = 0;
             bool stop = false;
+            // Lookahead (the claiming CTA): the next unit is claimed, and its unit and task
+            // records are loaded, while the current unit's copies are issued -- one dependent step
+            // per K tile -- so a new unit does not start with a chain of global round trips
+            // (claim, unit record, task record).  A CTA holds at most two claimed units, which it
+            // runs in claim order.
+            int nu = -1;
+            TcUnit nun{};
+            TcTask ntk{};
+            int nstate = 0;  // 0: nothing claimed, 1: claimed, 2: unit record loaded, 3: task loaded
+            auto advance = [&]() {
+                if (nstate == 0) {
+                    nu = atomicAdd(la.next_unit, 1);
+                } else if (nstate == 1) {
+                    if (nu >= la.nunits) nu = -1;
+                    if (nu >= 0) nun = la.units[nu];
+                } else if (nstate == 2) {
+                    if (nu >= 0) ntk = la.tasks[nun.task];
+                }
+                ++nstate;
+            };
             while (!stop && !*abort_word) {
                 int u, kt_unit = 0;
+                TcUnit un{};
+                TcTask t{};
                 if (!PAIR || issuer) {
-                    // claim the next unit and publish it to every reader
-                    u = atomicAdd(la.next_unit, 1);
-                    if (u >= la.nunits) u = -1;
+                    // take the claimed unit and publish it to every reader
+                    while (nstate < 3) advance();
+                    u = nu;
+                    un = nun;
+                    t = ntk;
+                    nstate = 0;
                     int kt_pub = 0;
                     if (u >= 0) {
-                        const TcUnit cu = la.units[u];
-                        kt_unit = cu.ktiles;
-                        kt_pub = cu.ktiles | (unit_parts(cu.chain) << 24);
+                        kt_unit = un.ktiles;
+                        kt_pub = un.ktiles | (unit_parts(un.chain) << 24);
                     }
                     const int i = (int)(slot % RING);
                     const uint32_t round = slot / RING;
@@ -493,9 +518,12 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                         raise_abort();
                         break;
                     }
+                    if (u >= 0) {
+                        un = la.units[u];
+                        t = la.tasks[un.task];
+                    }
                 }
                 if (u < 0) break;
-                const TcUnit un = la.units[u];
                 if (la.nlevels > 1) {
                     // a unit of a chained level reads what the previous level wrote: wait until
                     // every epilogue warp has finished every unit of that level
@@ -522,7 +550,6 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                         break;
                     }
                 }
-                const TcTask t = la.tasks[un.task];
                 const PlanArgs *pa = la.plans + t.plan;
                 const int NT = pa->NT;
                 const int cb = un.col * BN + (int)rank * C::B_ROWS;  // first B row staged here
@@ -533,8 +560,11 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                 const bool a_ok = !PAIR || issuer || t.m0 + 128 < t.M;
                 const int up = unit_parts(un.chain);
                 const uint32_t tx = (a_ok ? (uint32_t)up * TILE_BYTES : 0u) + (uint32_t)up * C::B_ROWS_BYTES;
+                TcItem it_next{};
+                if (t.nitem > 0) it_next = ti[0];
                 for (int q = 0; q < t.nitem && !stop; ++q) {
-                    const TcItem it = ti[q];
+                    const TcItem it = it_next;
+                    if (q + 1 < t.nitem) it_next = ti[q + 1];  // loaded while this item's copies go out
                     const uint8_t *a_pool = pa->pool[it.a_pool];
                     const uint8_t *b_pool = pa->buf[it.b_buf];
                     for (int kt = 0; kt < it.KT; ++kt, ++g) {
@@ -579,6 +609,7 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                                                  &full[s]);
                         }
                         filled[s] = round + 1;
+                        if ((!PAIR || issuer) && nstate < 3) advance();
                     }
                 }
             }
@@ -629,19 +660,24 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                     const uint32_t sa = tc::smem_u32(smem + s * C::STAGE);
                     const uint64_t da = tc::smem_desc_sw128(sa), db = tc::smem_desc_sw128(sa + C::A_BYTES);
                     const uint32_t dst = tmem + (uint32_t)(b * BN);
-                    uint32_t accum = first ? 0u : 1u;
+                    // the products of one K tile, fully unrolled for each product count (no
+                    // run-time loop bound between the MMAs)
+                    auto issue = [&](auto np) {
+                        uint32_t accum = first ? 0u : 1u;
 #pragma unroll
-                    for (int ks = 0; ks < 4; ++ks) {
+                        for (int ks = 0; ks < 4; ++ks) {
 #pragma unroll
-                        for (int j = 0; j < C::NPROD; ++j) {
-                            if (j >= nprod) break;
-                            const uint64_t ad = da + (uint64_t)((PA[j] * TILE_BYTES + ks * 32) >> 4);
-                            const uint64_t bd = db + (uint64_t)((PB[j] * C::B_ROWS_BYTES + ks * 32) >> 4);
-                            if constexpr (PAIR) tc::mma_bf16_pair(dst, ad, bd, IDESC, accum);
-                            else tc::mma_bf16(dst, ad, bd, IDESC, accum);
-                            accum = 1;
+                            for (int j = 0; j < decltype(np)::value; ++j) {
+                                const uint64_t ad = da + (uint64_t)((PA[j] * TILE_BYTES + ks * 32) >> 4);
+                                const uint64_t bd = db + (uint64_t)((PB[j] * C::B_ROWS_BYTES + ks * 32) >> 4);
+                                if constexpr (PAIR) tc::mma_bf16_pair(dst, ad, bd, IDESC, accum);
+                                else tc::mma_bf16(dst, ad, bd, IDESC, accum);
+                                accum = 1;
+                            }
                         }
-                    }
+                    };
+                    if (C::NPROD == 3 || nprod == 3) issue(std::integral_constant<int, 3>{});
+                    else issue(std::integral_constant<int, 6>{});
                     if constexpr (PAIR) {
                         tc::mma_commit_pair(&empty[s]);
                         if (last) tc::mma_commit_pair(&accf[b]);
@@ -965,13 +1001,15 @@ __global__ void __launch_bounds__(TcCfg<P, BN, STAGES_, PAIR>::THREADS, 1) tc_ge
                     for (int j = 0; j < 8; ++j) x[j] = acc[8 * g8 + j];
                     transpose8(x, lane);
                     const int n = col0 + 8 * g8 + (lane & 7);
-                    __nv_bfloat16 h[8], m[8], l[8];
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) tc::split3(x[j], h[j], m[j], l[j]);
+                    uint4 vh, vm, vl;
+                    tc::split3x8(x, vh, vm, vl);
                     if (k_ok) {
                         uint8_t *tile0 = tbuf + ((size_t)t.out_kt * NT + (size_t)(n >> 7) * KTv + kt) * 3 *
                                                     (size_t)TILE_BYTES;
-                        store_parts(tile0, 3, n & 127, (int)(kin >> 3), h, m, l);
+                        const uint32_t o = tc::swizzled_offset(n & 127, (int)kin);
+                        *reinterpret_cast<uint4 *>(tile0 + o) = vh;
+                        *reinterpret_cast<uint4 *>(tile0 + TILE_BYTES + o) = vm;
+                        *reinterpret_cast<uint4 *>(tile0 + 2 * TILE_BYTES + o) = vl;
                     }
                 }
             }
@@ -1885,13 +1923,18 @@ bool pairs_enabled()
     return on;
 }
 
-// MXB_TC_CHAIN=0 keeps every tree level in a launch of its own.
-
-// (read when an evaluation graph is built)
+// MXB_TC_CHAIN=0 keeps every tree level in a launch of its own; MXB_TC_CHAIN=2 chains every run
+// of sweep levels that share a product count and a tile, without timing the alternatives (read
+// when an evaluation graph is built).
 bool chains_enabled()
 {
     const char *e = getenv("MXB_TC_CHAIN");
     return !(e && *e == '0');
+}
+bool chains_forced()
+{
+    const char *e = getenv("MXB_TC_CHAIN");
+    return e && *e == '2';
 }
 
 // MXB_AUTOTUNE=0 keeps the default tiles (read when an evaluation graph is built).
@@ -2196,7 +2239,7 @@ int Batch::evaluate(const double *const *W, double *const *Y, const int *nrhs, i
             }
             tuned[nr] = bn;
         }
-        if (debug_flags & (MXB_DEBUG_CHAIN_LEVELS | MXB_DEBUG_STALL_LEVEL)) chain_all(bn);
+        if ((debug_flags & (MXB_DEBUG_CHAIN_LEVELS | MXB_DEBUG_STALL_LEVEL)) || chains_forced()) chain_all(bn);
         if (one_launch) {
             // one tile for the whole launch: the first tensor-core op's width, 64 or 128
             int w = 0;

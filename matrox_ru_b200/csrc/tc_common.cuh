@@ -347,5 +347,28 @@ __device__ __forceinline__ void split3(float x, __nv_bfloat16 &h, __nv_bfloat16 
     l = __float2bfloat16_rn(r2);
 }
 
+// Eight FP32 values -> their three bf16 parts, 16 bytes each (value e in bytes 2e, 2e + 1):
+// the same round-to-nearest splits as split3, two values per conversion.
+__device__ __forceinline__ void split3x8(const float (&x)[8], uint4 &h, uint4 &m, uint4 &l)
+{
+    uint32_t ph[4], pm[4], pl[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const float a = x[2 * i], b = x[2 * i + 1];
+        uint32_t p;
+        asm("cvt.rn.bf16x2.f32 %0, %1, %2;\n" : "=r"(p) : "f"(b), "f"(a));  // upper half: b
+        const float ra = a - __uint_as_float(p << 16), rb = b - __uint_as_float(p & 0xFFFF0000u);
+        ph[i] = p;
+        asm("cvt.rn.bf16x2.f32 %0, %1, %2;\n" : "=r"(p) : "f"(rb), "f"(ra));
+        const float sa = ra - __uint_as_float(p << 16), sb = rb - __uint_as_float(p & 0xFFFF0000u);
+        pm[i] = p;
+        asm("cvt.rn.bf16x2.f32 %0, %1, %2;\n" : "=r"(p) : "f"(sb), "f"(sa));
+        pl[i] = p;
+    }
+    h = make_uint4(ph[0], ph[1], ph[2], ph[3]);
+    m = make_uint4(pm[0], pm[1], pm[2], pm[3]);
+    l = make_uint4(pl[0], pl[1], pl[2], pl[3]);
+}
+
 }  // namespace tc
 }  // namespace mxb
