@@ -821,6 +821,12 @@ def main():
         "rel_err_vs_dense_64rows": {m: v.get("rel_err_vs_dense_64rows") for m, v in compact.items() if "ms" in v},
         "step_ms_min": head["step_ms_min"], "step_ms_max": head["step_ms_max"],
         "launch_sum_ms": compact[best]["launch_sum_ms"],
+        # each mode's whole-evaluation rate against its roofline: the FP64 mode against the cuBLAS
+        # DGEMM rate measured in this run, the split modes' executed bf16 products against the
+        # measured bf16 peak
+        "dgemm_tflops_measured": round(fp64_peak, 2),
+        "frac_of_peak": {m: round(v["executed_tflops"] / (fp64_peak if m == "fp64" else peaks["bf16_tflops"]), 4)
+                         for m, v in compact.items() if "ms" in v and v.get("executed_tflops")},
         "modes": compact, "detail": os.path.relpath(detail_path, ROOT), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
         "clocks": clocks, "cds_build_s": round(t_build, 1), "gpu_cds_blocks": gpu_blocks, "gpu_id_cds_build": gpu_id,
     }
