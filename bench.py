@@ -219,7 +219,9 @@ def c4_report(args):
     dev = torch.device("cuda", 0)
     t0 = time.time()
     X = S.gaussian_mixture(262144, 18, 32, -2.0, 2.0, 0.3, 1.0, seed=4)
-    cds = S.build_cds(X, S.KernelSpec("gaussian", 1.5), leaf_size=256, budget=0.03, tol=1e-5, max_rank=256, seed=6)
+    # per-node IDs factored on the GPU (the same ranks and skeletons as the host ID)
+    cds = S.build_cds(X, S.KernelSpec("gaussian", 1.5), leaf_size=256, budget=0.03, tol=1e-5, max_rank=256, seed=6,
+                      id_on_gpu=True)
     t_build = time.time() - t0
     r = 64
     flops = cds.flops(r)
@@ -269,6 +271,40 @@ def c4_report(args):
     grad64 = ev.adjoint(ev(Wd) - Yd)
     an = (grad64 * V).sum().item()
     peak = fp64_peak_tflops(torch, dev)
+    adj64 = ev.plan.adjoint(TG, r).clone()
+    # the same traversals on the tensor cores: a split-BF16 plan with its adjoint (MXB_PLAN_ADJOINT)
+    sev = H.Evaluator(cds, "split_bf16")
+    sfwd = timed(lambda: sev.plan.evaluate(TW, r, out=TY), args.steps)
+    sadj = timed(lambda: sev.plan.adjoint(TG, r, out=TY), args.steps)
+    sadj_err = float(torch.linalg.norm(sev.plan.adjoint(TG, r) - adj64) / torch.linalg.norm(adj64))
+    sfwd_err = float(torch.linalg.norm(sev.plan.evaluate(TW, r) - ev.plan.evaluate(TW, r)) /
+                     torch.linalg.norm(ev.plan.evaluate(TW, r)))
+
+    def sstep():
+        w = W.clone().requires_grad_()
+        loss = 0.5 * ((KernelMatVec.apply(w, sev) - Yt) ** 2).sum()
+        loss.backward()
+        return w.grad
+
+    sstep_ms = timed(sstep, args.steps)
+    sgrad = sstep()
+    sev.plan.status()
+    fb = cds.flops_breakdown(r)
+    exec_fl = 3 * (fb["near"] + fb["far"]) + 6 * fb["tree"]  # bf16 products of one traversal
+    bf16_peak = measured_peaks()[0]["bf16_tflops"]
+    split = {"forward_ms": round(sfwd, 3), "adjoint_ms": round(sadj, 3),
+             "loss_and_gradient_step_ms": round(sstep_ms, 3),
+             "forward_gflops": round(flops / (sfwd * 1e-3) / 1e9, 1),
+             "adjoint_gflops": round(flops / (sadj * 1e-3) / 1e9, 1),
+             "forward_rel_err_vs_fp64": sfwd_err, "adjoint_rel_err_vs_fp64": sadj_err,
+             "grad_rel_err_vs_fp64_adjoint": float(torch.linalg.norm(sgrad.double() - grad64) /
+                                                   torch.linalg.norm(grad64)),
+             "frac_of_bf16_peak": {"forward": round(exec_fl / (sfwd * 1e-3) / 1e12 / bf16_peak, 3),
+                                   "adjoint": round(exec_fl / (sadj * 1e-3) / 1e12 / bf16_peak, 3)},
+             "bf16_peak_tflops_measured": bf16_peak,
+             "precision": "bf16x3 near/far, bf16x6 transfers, FP32 accumulation, FP64 output; W, Y and the "
+                          "gradient FP32 at the torch boundary"}
+    del sev
     line = {"report": "differentiable kernel-ridge loss (c4)", "n": cds.n, "d": 18, "nrhs": r,
             "nleaf": cds.nleaf, "near_pairs": int(cds.ncount), "far_pairs": int(cds.fcount),
             "cds_gb_fp64": round(cds_bytes / 1e9, 2), "flops_per_traversal": flops,
@@ -285,6 +321,7 @@ def c4_report(args):
             "grad_rel_err_fd": abs(fd - an) / abs(an),
             "grad_fp32_vs_fp64_adjoint": float(torch.linalg.norm(grad32.double() - grad64) / torch.linalg.norm(grad64)),
             "precision": "FP64 traversals (forward and adjoint); W, Y and the gradient FP32 at the torch boundary",
+            "split_bf16": split,
             "cds_build_s": round(t_build, 1)}
     print(json.dumps(line), flush=True)
 

@@ -54,6 +54,11 @@ extern "C" {
                                  accuracy); FP64 final Y                                  */
 #define MXB_PREC_SPLIT_BF16_FAR6 2 /* as MXB_PREC_SPLIT_BF16 with 6-product far couplings */
 #define MXB_PREC_SPLIT_BF16_X6 3   /* 6 products (hi+mid+lo) for every GEMM               */
+/* OR'd into the precision of mxb_plan_create (no counterpart in the reference): a split-BF16
+ * plan also tiles the near blocks and far couplings transposed, so mxb_plan_adjoint runs the
+ * transposed traversal on the tensor cores with the plan's own product counts (the plan holds
+ * the near and far operand tiles twice).  FP64 plans always have the adjoint. */
+#define MXB_PLAN_ADJOINT 0x100
 
 /* ---- flags for the drop-ins ---------------------------------------------------------- */
 #define MXB_FLAG_MIRROR_WORKSPACES 1u /* copy wskel/uskel back to the caller's arrays    */
@@ -226,7 +231,8 @@ MXB_API int32_t mxb_plan_destroy(mxb_plan *plan);
 MXB_API int32_t mxb_plan_evaluate(mxb_plan *plan, const double *dW, double *dY, int32_t nrhs,
                           const int32_t *wptr, const int32_t *uptr, int32_t accumulate,
                           void *stream);
-/* dGW (+)= K~^T dG by the transposed traversal (no counterpart in the reference). */
+/* dGW (+)= K~^T dG by the transposed traversal (no counterpart in the reference).  FP64 plans,
+ * and split-BF16 plans created with MXB_PLAN_ADJOINT (MXB_ERR_UNSUPPORTED otherwise). */
 MXB_API int32_t mxb_plan_adjoint(mxb_plan *plan, const double *dG, double *dGW, int32_t nrhs,
                          const int32_t *gptr, const int32_t *gwptr, int32_t accumulate,
                          void *stream);
@@ -244,7 +250,7 @@ MXB_API int32_t mxb_plan_set_permutation(mxb_plan *plan, const int32_t *perm);
 MXB_API int32_t mxb_plan_evaluate_ordered(mxb_plan *plan, const double *dW, int64_t w_rs, int64_t w_cs,
                                           double *dY, int64_t y_rs, int64_t y_cs, int32_t nrhs,
                                           int32_t accumulate, void *stream);
-/* dGW (+)= K~^T dG in the caller's point order (FP64 plans; permuted copies). */
+/* dGW (+)= K~^T dG in the caller's point order (permuted copies; the plans mxb_plan_adjoint takes). */
 MXB_API int32_t mxb_plan_adjoint_ordered(mxb_plan *plan, const double *dG, int64_t g_rs, int64_t g_cs,
                                          double *dGW, int64_t gw_rs, int64_t gw_cs, int32_t nrhs,
                                          int32_t accumulate, void *stream);

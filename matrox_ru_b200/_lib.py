@@ -32,6 +32,7 @@ DEBUG_STALL_LEVEL = 4
 DEBUG_ONE_LAUNCH = 8
 BATCH_LEVEL_LAUNCHES, BATCH_ONE_LAUNCH = 0, 1
 TILE_PAIR = 4096
+PLAN_ADJOINT = 0x100  # MXB_PLAN_ADJOINT: OR'd into the precision of mxb_plan_create
 KERNEL_KINDS = {"gaussian": 0, "imq": 1, "newton": 2}
 PHASES = {0: "split_w", 1: "up", 2: "far", 3: "down", 4: "near", 5: "leaf_down", 6: "far_down",
           7: "near_leaf_down", 8: "far_near"}

@@ -391,12 +391,15 @@ uint64_t Plan::flops(int nrhs) const
 
 int Plan::create(const mxb_cds_desc &d, int prec, Plan **out)
 {
-    if (prec < MXB_PREC_FP64 || prec > MXB_PREC_SPLIT_BF16_X6) {
+    const int flags = prec & ~0xFF;
+    prec &= 0xFF;
+    if (prec < MXB_PREC_FP64 || prec > MXB_PREC_SPLIT_BF16_X6 || (flags & ~MXB_PLAN_ADJOINT)) {
         set_error("unknown precision mode");
         return MXB_ERR_ARG;
     }
     std::unique_ptr<Plan> p(new Plan());
     p->precision = prec;
+    p->want_adjoint = (flags & MXB_PLAN_ADJOINT) && prec != MXB_PREC_FP64;  // FP64 plans always have it
     MXB_CUDA(cudaGetDevice(&p->device));
     int rc = p->validate(d);
     if (rc) return rc;

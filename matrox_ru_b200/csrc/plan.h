@@ -24,6 +24,7 @@ struct Plan : public mxb_plan {
     // ---- host structure ----
     int device = 0;
     int precision = MXB_PREC_FP64;
+    bool want_adjoint = false;  // split-BF16: also tile the transposed operands (MXB_PLAN_ADJOINT)
     int nleaf = 0, numnodes = 0, is_hss = 0, root = 0;
     std::vector<int> Ddim, slen, lch, rch, lm, parent, depth, height, bfs;
     std::vector<int32_t> VTptr;

@@ -61,7 +61,8 @@ namespace {
 
 using tc::TILE_BYTES;
 
-enum APool { POOL_NEAR, POOL_FAR, POOL_VU3, POOL_VD3, NPOOL };
+// POOL_NEART / POOL_FART: the near blocks and far couplings transposed (plans with the adjoint)
+enum APool { POOL_NEAR, POOL_FAR, POOL_VU3, POOL_VD3, POOL_NEART, POOL_FART, NPOOL };
 enum BBuf { BUF_W, BUF_WSKEL, BUF_USKEL, NBUF };
 
 struct TcItem {
@@ -1191,16 +1192,19 @@ struct SplitBF16 {
     uint8_t *pool[NPOOL] = {};
     size_t pool_bytes[NPOOL] = {};
     std::vector<Op> ops;
+    std::vector<Op> ops_adj;  // the transposed traversal (plans created with MXB_PLAN_ADJOINT)
     std::vector<TcTask> tasks;
     std::vector<TcItem> items;
     std::vector<SplitJob> jobs;
     std::vector<int64_t> leaf_kt, node_kt;  // K-tile bases
     int64_t leaf_kt_total = 0, node_kt_total = 0;
     int nt_cap = 0, nrhs_cap = 0;
+    int buf_gen = 0;  // counts reallocations of the buffers below (graphs hold their addresses)
     uint8_t *Wt = nullptr, *wT = nullptr, *uT = nullptr;
     float *u32 = nullptr;  // FP32 far results awaiting the down launch
     int *dErr = nullptr;
-    Batch *self = nullptr;  // the single-plan batch used by mxb_plan_evaluate
+    Batch *self = nullptr;      // the single-plan batch used by mxb_plan_evaluate
+    Batch *self_adj = nullptr;  // the same for mxb_plan_adjoint
 };
 
 // ---------------------------------------------------------------------------------------
@@ -1252,6 +1256,9 @@ struct Batch : public mxb_batch {
     };
     std::vector<Entry> entries;
     std::map<std::vector<int>, std::vector<int>> tuned;  // nrhs signature -> bn per op
+    // buffer generation of each plan when the entries were captured: another batch of the same
+    // plan (its own single-plan batch, its adjoint's, a user batch) may have reallocated them
+    std::vector<int> buf_gens;
     cudaStream_t capture_stream = nullptr;
     int device = 0;
 
@@ -1278,7 +1285,7 @@ struct Batch : public mxb_batch {
         for (Entry &e : entries) release(e);
         entries.clear();
     }
-    int build(const std::vector<Plan *> &ps);
+    int build(const std::vector<Plan *> &ps, bool adjoint = false);
     int evaluate(const double *const *W, double *const *Y, const int *nrhs, int accumulate, cudaStream_t stream,
                  int debug_flags, long long wait_cycles, const CallerOrder *order = nullptr);
     int enqueue(Entry &e, cudaStream_t stream, int debug_flags, long long wait_cycles, const std::vector<int> &bn,
@@ -1296,7 +1303,7 @@ struct Batch : public mxb_batch {
                 int cap, int *nops);
 };
 
-int Batch::build(const std::vector<Plan *> &ps)
+int Batch::build(const std::vector<Plan *> &ps, bool adjoint)
 {
     if (ps.empty()) return batch_fail("empty batch");
     plans = ps;
@@ -1308,8 +1315,10 @@ int Batch::build(const std::vector<Plan *> &ps)
     }
     // merge ops by key, in key order; tasks and jobs get their plan index and offsets
     std::map<int64_t, std::vector<std::pair<int, const Op *>>> by_key;
-    for (int pi = 0; pi < (int)ps.size(); ++pi)
-        for (const Op &o : ps[pi]->bf16->ops) by_key[o.key].push_back({pi, &o});
+    for (int pi = 0; pi < (int)ps.size(); ++pi) {
+        if (adjoint && ps[pi]->bf16->ops_adj.empty()) return batch_fail("the plan has no split-BF16 adjoint");
+        for (const Op &o : adjoint ? ps[pi]->bf16->ops_adj : ps[pi]->bf16->ops) by_key[o.key].push_back({pi, &o});
+    }
     for (auto &kv : by_key) {
         MOp m{};
         m.key = kv.first;
@@ -1878,6 +1887,7 @@ int split_buffers(Plan &p, SplitBF16 &S, int nrhs)
     if (rc) return rc;
     S.nt_cap = NT;
     S.nrhs_cap = nrhs;
+    ++S.buf_gen;
     return MXB_OK;
 }
 
@@ -2165,12 +2175,13 @@ int Batch::evaluate(const double *const *W, double *const *Y, const int *nrhs, i
     std::vector<int> nr(nrhs, nrhs + np);
     if (one_launch && order) return batch_fail("the one-launch mode takes leaf-blocked W and Y", MXB_ERR_UNSUPPORTED);
     bool realloc = false;
+    if (buf_gens.size() != (size_t)np) buf_gens.assign(np, -1);
     for (int i = 0; i < np; ++i) {
         if (nr[i] < 1 || !W[i] || !Y[i]) return batch_fail("bad operand or nrhs in batch");
-        const int nt0 = plans[i]->bf16->nt_cap, nr0 = plans[i]->bf16->nrhs_cap;
         int rc = split_buffers(*plans[i], *plans[i]->bf16, nr[i]);
         if (rc) return rc;
-        realloc |= plans[i]->bf16->nt_cap != nt0 || plans[i]->bf16->nrhs_cap != nr0;
+        realloc |= plans[i]->bf16->buf_gen != buf_gens[i];
+        buf_gens[i] = plans[i]->bf16->buf_gen;
     }
     if (realloc) clear();
     MXB_CUDA_OR(configure_all_tc());
@@ -2443,6 +2454,17 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
         near_a[k] = add_pool(POOL_NEAR, 0, near_off[k], Ddim[near_x[k]], Ddim[near_x[k]], Ddim[near_y[k]], 0, near_parts);
     for (size_t k = 0; k < far_x.size(); ++k)
         far_a[k] = add_pool(POOL_FAR, 1, far_off[k], slen[far_x[k]], slen[far_x[k]], slen[far_y[k]], 0, far_parts);
+    // the adjoint's operands: D_xy^T (m_y x m_x) and B_xy^T (s_y x s_x)
+    std::vector<uint64_t> neart_a, fart_a;
+    if (want_adjoint) {
+        neart_a.resize(near_x.size());
+        fart_a.resize(far_x.size());
+        for (size_t k = 0; k < near_x.size(); ++k)
+            neart_a[k] = add_pool(POOL_NEART, 0, near_off[k], Ddim[near_x[k]], Ddim[near_y[k]], Ddim[near_x[k]], 1,
+                                  near_parts);
+        for (size_t k = 0; k < far_x.size(); ++k)
+            fart_a[k] = add_pool(POOL_FART, 1, far_off[k], slen[far_x[k]], slen[far_y[k]], slen[far_x[k]], 1, far_parts);
+    }
     std::vector<uint64_t> up_a(numnodes), up_b(numnodes), down_a(numnodes);
     for (int v = 0; v < numnodes; ++v) {
         if (!projects(v)) continue;
@@ -2494,6 +2516,7 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
         maxh = std::max(maxh, height[v]);
         maxd = std::max(maxd, depth[v]);
     }
+    std::vector<Op> *op_list = &S->ops;  // the forward's, then the adjoint's
     auto begin_op = [&](int phase, int level, int P) {
         Op o{};
         o.key = op_key(phase, level, P);
@@ -2501,12 +2524,12 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
         o.level = level;
         o.P = P;
         o.first = phase == PH_SPLITW ? (int)S->jobs.size() : (int)S->tasks.size();
-        S->ops.push_back(o);
+        op_list->push_back(o);
     };
     auto end_op = [&]() {
-        Op &o = S->ops.back();
+        Op &o = op_list->back();
         o.count = (o.phase == PH_SPLITW ? (int)S->jobs.size() : (int)S->tasks.size()) - o.first;
-        if (o.count == 0) S->ops.pop_back();
+        if (o.count == 0) op_list->pop_back();
     };
     auto add_tasks = [&](int16_t out_kind, int64_t c_row, int64_t out_kt, int ldc, int M, int item0,
                          int16_t beta, int t_buf) {
@@ -2621,6 +2644,46 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
     }
     end_op();
 
+    // ---- the transposed traversal (dGW = K~^T dG) ----
+    // The same W split, up sweep, down sweep and leaf down; the far couplings and the near field
+    // transposed: far pair (x, y) adds B_xy^T wskel[x] to node y, near pair (x, y) adds
+    // D_xy^T G[x] to leaf y (the FP64 adjoint's traversal, with the transposed tiled pools).
+    if (want_adjoint) {
+        op_list = &S->ops_adj;
+        for (const Op &o : S->ops)
+            if (o.phase == PH_SPLITW || o.phase == PH_UP || o.phase == PH_DOWN || o.phase == PH_LEAFDOWN)
+                S->ops_adj.push_back(o);
+        std::vector<std::vector<int>> far_in(numnodes), near_in(nleaf);
+        for (size_t k = 0; k < far_x.size(); ++k) far_in[far_y[k]].push_back((int)k);
+        for (size_t k = 0; k < near_x.size(); ++k) near_in[near_y[k]].push_back((int)k);
+        auto near_tasks_t = [&]() {
+            for (int v : bfs) {
+                if (lch[v] != -1) continue;
+                const int x = lm[v];
+                const int item0 = (int)S->items.size();
+                for (int k : near_in[x]) item(POOL_NEART, neart_a[k], BUF_W, S->leaf_kt[near_x[k]], Ddim[near_x[k]]);
+                add_tasks(OUT_Y, x, 0, Ddim[x], Ddim[x], item0, 2, BUF_W);
+            }
+        };
+        begin_op(near_with_far ? PH_FARNEAR : PH_FAR, 0, far_parts);
+        for (int c : bfs) {
+            if (!projects(c)) continue;
+            const int item0 = (int)S->items.size();
+            for (int k : far_in[c])
+                if (slen[far_x[k]] > 0) item(POOL_FART, fart_a[k], BUF_WSKEL, S->node_kt[far_x[k]], slen[far_x[k]]);
+            add_tasks(has_down(c) ? OUT_F32 : OUT_TILES, skel_row[c], S->node_kt[c], slen[c], slen[c], item0, 0,
+                      BUF_USKEL);
+        }
+        if (near_with_far) near_tasks_t();
+        end_op();
+        if (!near_with_far) {
+            begin_op(PH_NEAR, 0, near_parts);
+            near_tasks_t();
+            end_op();
+        }
+        op_list = &S->ops;
+    }
+
     // the split path reads only the tiled pools: release the FP64 copies of the CDS
     const uint64_t fp64_len[3] = {D_len, B_len, VT_len};
     double **fp64_buf[3] = {&dD, &dB, &dVT};
@@ -2640,24 +2703,35 @@ int Plan::setup_split_bf16(const mxb_cds_desc &)
     }
     // the batch of this plan alone, used by mxb_plan_evaluate
     S->self = new Batch();
-    return S->self->build({this});
+    rc = S->self->build({this});
+    if (!rc && want_adjoint) {
+        S->self_adj = new Batch();
+        rc = S->self_adj->build({this}, true);
+    }
+    return rc;
 }
 
 int Plan::run_split_bf16(const std::vector<Launch> &L, const double *dW, double *dY, int nrhs, int accumulate,
                          cudaStream_t stream, const CallerOrder *order)
 {
+    Batch *b = bf16->self;
     if (&L == &launches_adj) {
-        set_error("the adjoint runs in FP64 mode only (create an FP64 plan for mxb_plan_adjoint)");
-        return MXB_ERR_UNSUPPORTED;
+        if (!bf16->self_adj) {
+            set_error("this split-BF16 plan has no adjoint: create it with precision | MXB_PLAN_ADJOINT (or use an "
+                      "FP64 plan)");
+            return MXB_ERR_UNSUPPORTED;
+        }
+        b = bf16->self_adj;
     }
-    const int rc = batch_set_one_launch(bf16->self, (debug_flags & MXB_DEBUG_ONE_LAUNCH) != 0);
+    const int rc = batch_set_one_launch(b, (debug_flags & MXB_DEBUG_ONE_LAUNCH) != 0);
     if (rc) return rc;
-    return bf16->self->evaluate(&dW, &dY, &nrhs, accumulate, stream, debug_flags, debug_wait_cycles, order);
+    return b->evaluate(&dW, &dY, &nrhs, accumulate, stream, debug_flags, debug_wait_cycles, order);
 }
 
 void Plan::clear_split_graphs()
 {
     if (bf16 && bf16->self) bf16->self->clear();
+    if (bf16 && bf16->self_adj) bf16->self_adj->clear();
 }
 
 int split_bf16_prepare() { return configure_all_tc() == cudaSuccess ? MXB_OK : MXB_ERR_CUDA; }
@@ -2700,7 +2774,10 @@ int split_bf16_status(Plan &p)
 
 void Plan::free_split_bf16()
 {
-    if (bf16) delete bf16->self;
+    if (bf16) {
+        delete bf16->self;
+        delete bf16->self_adj;
+    }
     delete bf16;
     bf16 = nullptr;
 }

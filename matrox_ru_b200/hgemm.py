@@ -295,9 +295,11 @@ def batched_id(pool, shapes, tol: float, max_rank: int, stream=None):
 class Plan:
     """Device-resident CDS and task lists (``mxb_plan_*``).  ``pools`` optionally gives the
     numeric pools (D, B, VT) as CUDA tensors (e.g. from :func:`kernel_blocks`) instead of the
-    CDS's host arrays."""
+    CDS's host arrays.  ``adjoint``: a split-BF16 plan also tiles the transposed near blocks and
+    far couplings, so :meth:`adjoint` runs on the tensor cores (``MXB_PLAN_ADJOINT``); FP64 plans
+    always have the adjoint."""
 
-    def __init__(self, cds, precision: str = "fp64", pools=None):
+    def __init__(self, cds, precision: str = "fp64", pools=None, adjoint: bool = False):
         torch = _torch()
         if not torch.cuda.is_available():
             raise RuntimeError("matrox_ru_b200.Plan needs a CUDA device")
@@ -316,7 +318,8 @@ class Plan:
                 setattr(desc, name, t.data_ptr())
             torch.cuda.synchronize()  # the pools were written on torch's stream
         h = P()
-        check(lib.mxb_plan_create(ctypes.byref(desc), PRECISIONS[precision], ctypes.byref(h)), "mxb_plan_create")
+        code = PRECISIONS[precision] | (_lib.PLAN_ADJOINT if adjoint and precision != "fp64" else 0)
+        check(lib.mxb_plan_create(ctypes.byref(desc), code, ctypes.byref(h)), "mxb_plan_create")
         self._h = h
         self.cds = cds
         self.precision = precision
@@ -415,7 +418,8 @@ class Plan:
                              accumulate, stream)
 
     def adjoint_ordered(self, G, out=None, accumulate: bool = False, stream=None):
-        """out (+)= K~^T G in the caller's point order (FP64 plans)."""
+        """out (+)= K~^T G in the caller's point order (FP64 plans, split-BF16 plans with the
+        adjoint)."""
         return self._ordered(_lib.load().mxb_plan_adjoint_ordered, "mxb_plan_adjoint_ordered", G, out,
                              accumulate, stream)
 
@@ -511,7 +515,8 @@ class Evaluator:
 
     def __init__(self, cds, precision: str = "fp64", plan: Optional[Plan] = None):
         torch = _torch()
-        self.plan = plan if plan is not None else Plan(cds, precision)
+        # a split-BF16 evaluator carries the tensor-core adjoint too (its backward pass)
+        self.plan = plan if plan is not None else Plan(cds, precision, adjoint=True)
         self.plan.set_permutation(cds.perm)
         self.cds = cds
         dev = torch.device("cuda", self.plan.device)
