@@ -339,7 +339,7 @@ def tolerance_sweep(args, cfg):
     r = cfg["nrhs"]
     for tol in (1e-3, 1e-5, 1e-7):
         cds = S.build_cds(X, spec, leaf_size=cfg["leaf"], budget=cfg["budget"], tol=tol, max_rank=cfg["max_rank"],
-                          seed=cfg["seed"])
+                          seed=cfg["seed"], id_on_gpu=True)
         g = torch.Generator(device=dev).manual_seed(cfg["seed"] + 1)
         TW = torch.randn(cds.n * r, dtype=torch.float64, device=dev, generator=g)
         rows = np.random.default_rng(0).choice(cds.n, 64, replace=False)
