@@ -87,6 +87,20 @@ MXB_API int32_t mxb_cache_invalidate(void);
 #define MXB_CACHE_OFF 2
 MXB_API int32_t mxb_cache_set_mode(int32_t mode);
 
+/* Test hook, no counterpart in the reference (host code only, no device needed): the unit order
+ * that a chained tree sweep runs in when its units wait on per-node counters, for a synthetic
+ * dependency forest.  Node i reads the outputs of nodes deps[dep_first[i] .. dep_first[i + 1])
+ * (at most two; dep_first has nnodes + 1 entries), has ntask[i] row tiles of kt[i] K tiles and
+ * ncol column tiles, and `workers` CTAs claim the units.  Unit u (u < *count <= cap) is written as
+ * its node, its column tile, the counters it waits for (dep0, dep1; -1: none) with the units each
+ * must count (need: low and high 16 bits) and the counter it signals (sig; -1: none).
+ * MXB_ERR_UNSUPPORTED when the dependencies are not a tree (the sweep then keeps level
+ * barriers). */
+MXB_API int32_t mxb_debug_dataflow_order(int32_t nnodes, const int32_t *dep_first, const int32_t *deps,
+                                         const int32_t *ntask, const int32_t *kt, int32_t ncol, int32_t workers,
+                                         int32_t *node, int32_t *col, int32_t *dep0, int32_t *dep1,
+                                         int32_t *need, int32_t *sig, int64_t cap, int64_t *count);
+
 /* ---- drop-ins: H2-b -------------------------------------------------------------------- */
 
 /* Replaces CBHGEMM, codeGen/H2GEMM.h:380-389 (coarsened + blocked H2-b evaluation).

@@ -96,6 +96,8 @@ def load(path: str = LIB_PATH):
     lib.mxb_set_precision.argtypes = [I32]
     lib.mxb_set_flags.argtypes = [U32]
     lib.mxb_cache_set_mode.argtypes = [I32]
+    lib.mxb_debug_dataflow_order.argtypes = [I32, P, P, P, P, I32, I32, P, P, P, P, P, P, I64,
+                                             ctypes.POINTER(I64)]
     lib.mxb_batch_set_launch_mode.argtypes = [P, I32]
     lib.mxb_plan_create.argtypes = [ctypes.POINTER(CdsDesc), I32, ctypes.POINTER(P)]
     lib.mxb_plan_destroy.argtypes = [P]

@@ -1445,6 +1445,141 @@ bool dataflow_enabled()
     return !(e && *e == '0');
 }
 
+// A node of a chained sweep: the tasks of one output block (its row tiles).
+struct DfNode {
+    int plan = 0, level = 0;
+    int64_t key = 0;         // tile K base of the output (OUT_TILES) or leaf index (OUT_Y)
+    std::vector<int> tasks;  // tasks that carry units (row tiles; the even one of a pair)
+    std::vector<int> dep;    // nodes whose output tiles this node reads
+    std::vector<int> cons;   // nodes that read this node's output tiles
+    int ncol = 0, kt = 0, ctr = -1, order = 0, unplaced = 0;
+    double ready = 0, finish = 0;
+};
+
+// The dataflow order of a run's nodes (their dep lists filled): depth-first order over the tree,
+// counters from `ndeps` on, and the list-scheduling simulation that emits the units (the scheme
+// is described at Batch::dataflow_units).  unit_node, if given, receives the node of every emitted unit.
+// Returns 1, 0 where the dependencies are not a tree (nothing emitted), or an error code.
+int dataflow_schedule(std::vector<DfNode> &nodes, int workers, std::vector<TcUnit> &units, int &ndeps,
+                      std::vector<int> *unit_node = nullptr)
+{
+    for (const DfNode &nd : nodes)
+        if (nd.tasks.empty() || nd.dep.size() > 2 || nd.tasks.size() > 0xFFFF) return 0;
+    for (DfNode &nd : nodes) nd.cons.clear();
+    for (int n = 0; n < (int)nodes.size(); ++n)
+        for (int wn : nodes[n].dep) {
+            if (wn < 0 || wn >= (int)nodes.size() || wn == n) return 0;
+            nodes[wn].cons.push_back(n);
+        }
+    bool in_tree = true, out_tree = true;
+    for (const DfNode &nd : nodes) {
+        in_tree &= nd.cons.size() <= 1;
+        out_tree &= nd.dep.size() <= 1;
+    }
+    if (!in_tree && !out_tree) return 0;
+
+    // depth-first order: children before parents (up sweep), parents before children (down)
+    auto tree_less = [&](int a, int b) {
+        return std::tie(nodes[a].plan, nodes[a].level, nodes[a].key) < std::tie(nodes[b].plan, nodes[b].level, nodes[b].key);
+    };
+    int next = 0;
+    std::vector<int> roots;
+    for (int n = 0; n < (int)nodes.size(); ++n)
+        if (in_tree ? nodes[n].cons.empty() : nodes[n].dep.empty()) roots.push_back(n);
+    std::sort(roots.begin(), roots.end(), tree_less);
+    std::vector<char> seen(nodes.size(), 0);
+    bool cyclic = false;
+    std::function<void(int)> visit = [&](int n) {
+        if (seen[n]) {
+            cyclic = true;
+            return;
+        }
+        seen[n] = 1;
+        std::vector<int> ch = in_tree ? nodes[n].dep : nodes[n].cons;
+        std::sort(ch.begin(), ch.end(), tree_less);
+        if (!in_tree) nodes[n].order = next++;
+        for (int c : ch) visit(c);
+        if (in_tree) nodes[n].order = next++;
+    };
+    for (int r : roots) visit(r);
+    if (cyclic || next != (int)nodes.size()) return 0;
+
+    for (DfNode &nd : nodes)
+        if (!nd.cons.empty()) {
+            nd.ctr = ndeps;
+            ndeps += nd.ncol;
+        }
+
+    // list scheduling (simulated, time in K tiles): one worker per CTA (pair), which claims its
+    // next unit once it has issued the last loads of the current one, i.e. about STAGES K
+    // tiles before the current unit's MMAs end -- a unit claimed before its inputs are written
+    // holds its CTA until they are
+    struct Cta {
+        double claim, mma_free;
+        bool operator>(const Cta &o) const { return claim > o.claim; }
+    };
+    std::priority_queue<Cta, std::vector<Cta>, std::greater<Cta>> ctas;
+    for (int i = 0; i < std::max(1, workers); ++i) ctas.push(Cta{0.0, 0.0});
+    constexpr double STAGES_KT = 2.0;
+    auto later_order = [&](int a, int b) { return nodes[a].order > nodes[b].order; };
+    auto later_ready = [&](int a, int b) { return nodes[a].ready > nodes[b].ready; };
+    std::priority_queue<int, std::vector<int>, decltype(later_order)> ready(later_order);
+    std::priority_queue<int, std::vector<int>, decltype(later_ready)> waiting(later_ready);
+    for (int n = 0; n < (int)nodes.size(); ++n) {
+        nodes[n].ready = nodes[n].finish = 0;
+        nodes[n].unplaced = (int)nodes[n].dep.size();
+        if (!nodes[n].unplaced) waiting.push(n);
+    }
+    for (size_t placed = 0; placed < nodes.size(); ++placed) {
+        const double now = ctas.top().claim;
+        while (!waiting.empty() && nodes[waiting.top()].ready <= now) {
+            ready.push(waiting.top());
+            waiting.pop();
+        }
+        int g;
+        if (!ready.empty()) {
+            g = ready.top();
+            ready.pop();
+        } else if (!waiting.empty()) {
+            g = waiting.top();  // nothing ready: the node whose inputs finish first
+            waiting.pop();
+        } else {
+            return batch_fail("dataflow schedule: a node's inputs are never written");
+        }
+        DfNode &nd = nodes[g];
+        int need = 0;
+        for (size_t d = 0; d < nd.dep.size(); ++d) need |= (int)nodes[nd.dep[d]].tasks.size() << (16 * d);
+        for (int c = 0; c < nd.ncol; ++c)
+            for (int t : nd.tasks) {
+                Cta w = ctas.top();
+                ctas.pop();
+                const double load = std::max(w.claim, nd.ready);  // the producer waits for inputs
+                const double mma = std::max(load + 1.0, w.mma_free);
+                w.mma_free = mma + nd.kt;
+                w.claim = std::max(load, mma + std::max(0.0, nd.kt - STAGES_KT));
+                ctas.push(w);
+                nd.finish = std::max(nd.finish, mma + nd.kt + 1.0);
+                TcUnit u{};
+                u.task = t;
+                u.col = c;
+                u.ktiles = nd.kt;
+                u.chain = 0;
+                u.dep0 = nd.dep.size() > 0 ? nodes[nd.dep[0]].ctr + c : -1;
+                u.dep1 = nd.dep.size() > 1 ? nodes[nd.dep[1]].ctr + c : -1;
+                u.need = need;
+                u.sig = nd.ctr >= 0 ? nd.ctr + c : -1;
+                units.push_back(u);
+                if (unit_node) unit_node->push_back(g);
+            }
+        for (int cn : nd.cons) {
+            DfNode &cd = nodes[cn];
+            cd.ready = std::max(cd.ready, nd.finish);
+            if (--cd.unplaced == 0) waiting.push(cn);
+        }
+    }
+    return 1;
+}
+
 // Dataflow schedule of a chained run of sweep ops [k, end): the up-sweep heights, or the
 // down-sweep depths with leaf down.  A node (the tasks of one output block: its row tiles)
 // depends on the nodes of earlier levels of the run whose output tiles its items read, and
@@ -1470,16 +1605,7 @@ int Batch::dataflow_units(const Entry &e, size_t k, size_t end, const std::vecto
 {
     const bool pair = tile_pair(bn[k]);
     const int w = tile_width(bn[k]);
-    struct Node {
-        int plan = 0, level = 0;
-        int64_t key = 0;         // tile K base of the output (OUT_TILES) or leaf index (OUT_Y)
-        std::vector<int> tasks;  // tasks that carry units (row tiles; the even one of a pair)
-        std::vector<int> dep;    // nodes whose output tiles this node reads
-        std::vector<int> cons;   // nodes that read this node's output tiles
-        int ncol = 0, kt = 0, ctr = -1, order = 0, unplaced = 0;
-        double ready = 0, finish = 0;
-    };
-    std::vector<Node> nodes;
+    std::vector<DfNode> nodes;
     std::map<std::tuple<int, int, int64_t>, int> by_out;  // (plan, tile buffer or -1 for Y, key)
     for (size_t q = k; q < end; ++q) {
         const MOp &m = ops[q];
@@ -1494,7 +1620,7 @@ int Batch::dataflow_units(const Entry &e, size_t k, size_t end, const std::vecto
             if (it == by_out.end()) {
                 n = (int)nodes.size();
                 by_out[id] = n;
-                Node nd;
+                DfNode nd;
                 nd.plan = tk.plan;
                 nd.level = (int)q;
                 nd.key = std::get<2>(id);
@@ -1509,7 +1635,7 @@ int Batch::dataflow_units(const Entry &e, size_t k, size_t end, const std::vecto
         }
     }
     for (int n = 0; n < (int)nodes.size(); ++n) {
-        Node &nd = nodes[n];
+        DfNode &nd = nodes[n];
         if (nd.tasks.empty()) return 0;
         const TcTask &t0 = tasks[nd.tasks[0]];
         for (int q = t0.item0; q < t0.item0 + t0.nitem; ++q) nd.kt += items[q].KT;
@@ -1523,109 +1649,8 @@ int Batch::dataflow_units(const Entry &e, size_t k, size_t end, const std::vecto
                 if (std::find(nd.dep.begin(), nd.dep.end(), wn) == nd.dep.end()) nd.dep.push_back(wn);
             }
         }
-        if (nd.dep.size() > 2 || nd.tasks.size() > 0xFFFF) return 0;
     }
-    for (int n = 0; n < (int)nodes.size(); ++n)
-        for (int wn : nodes[n].dep) nodes[wn].cons.push_back(n);
-    bool in_tree = true, out_tree = true;
-    for (const Node &nd : nodes) {
-        in_tree &= nd.cons.size() <= 1;
-        out_tree &= nd.dep.size() <= 1;
-    }
-    if (!in_tree && !out_tree) return 0;
-
-    // depth-first order: children before parents (up sweep), parents before children (down)
-    auto tree_less = [&](int a, int b) {
-        return std::tie(nodes[a].plan, nodes[a].level, nodes[a].key) < std::tie(nodes[b].plan, nodes[b].level, nodes[b].key);
-    };
-    int next = 0;
-    std::vector<int> roots;
-    for (int n = 0; n < (int)nodes.size(); ++n)
-        if (in_tree ? nodes[n].cons.empty() : nodes[n].dep.empty()) roots.push_back(n);
-    std::sort(roots.begin(), roots.end(), tree_less);
-    std::function<void(int)> visit = [&](int n) {
-        std::vector<int> ch = in_tree ? nodes[n].dep : nodes[n].cons;
-        std::sort(ch.begin(), ch.end(), tree_less);
-        if (!in_tree) nodes[n].order = next++;
-        for (int c : ch) visit(c);
-        if (in_tree) nodes[n].order = next++;
-    };
-    for (int r : roots) visit(r);
-    if (next != (int)nodes.size()) return 0;
-
-    for (Node &nd : nodes)
-        if (!nd.cons.empty()) {
-            nd.ctr = ndeps;
-            ndeps += nd.ncol;
-        }
-
-    // list scheduling (simulated, time in K tiles): one worker per CTA (pair), which claims its
-    // next unit once it has issued the last loads of the current one, i.e. about STAGES K
-    // tiles before the current unit's MMAs end -- a unit claimed before its inputs are written
-    // holds its CTA until they are
-    const int workers = std::max(1, pair ? sm_count() / 2 : sm_count());
-    struct Cta {
-        double claim, mma_free;
-        bool operator>(const Cta &o) const { return claim > o.claim; }
-    };
-    std::priority_queue<Cta, std::vector<Cta>, std::greater<Cta>> ctas;
-    for (int i = 0; i < workers; ++i) ctas.push(Cta{0.0, 0.0});
-    constexpr double STAGES_KT = 2.0;
-    auto later_order = [&](int a, int b) { return nodes[a].order > nodes[b].order; };
-    auto later_ready = [&](int a, int b) { return nodes[a].ready > nodes[b].ready; };
-    std::priority_queue<int, std::vector<int>, decltype(later_order)> ready(later_order);
-    std::priority_queue<int, std::vector<int>, decltype(later_ready)> waiting(later_ready);
-    for (int n = 0; n < (int)nodes.size(); ++n) {
-        nodes[n].unplaced = (int)nodes[n].dep.size();
-        if (!nodes[n].unplaced) waiting.push(n);
-    }
-    for (size_t placed = 0; placed < nodes.size(); ++placed) {
-        const double now = ctas.top().claim;
-        while (!waiting.empty() && nodes[waiting.top()].ready <= now) {
-            ready.push(waiting.top());
-            waiting.pop();
-        }
-        int g;
-        if (!ready.empty()) {
-            g = ready.top();
-            ready.pop();
-        } else if (!waiting.empty()) {
-            g = waiting.top();  // nothing ready: the node whose inputs finish first
-            waiting.pop();
-        } else {
-            return batch_fail("dataflow schedule: a node's inputs are never written");
-        }
-        Node &nd = nodes[g];
-        int need = 0;
-        for (size_t d = 0; d < nd.dep.size(); ++d) need |= (int)nodes[nd.dep[d]].tasks.size() << (16 * d);
-        for (int c = 0; c < nd.ncol; ++c)
-            for (int t : nd.tasks) {
-                Cta w = ctas.top();
-                ctas.pop();
-                const double load = std::max(w.claim, nd.ready);  // the producer waits for inputs
-                const double mma = std::max(load + 1.0, w.mma_free);
-                w.mma_free = mma + nd.kt;
-                w.claim = std::max(load, mma + std::max(0.0, nd.kt - STAGES_KT));
-                ctas.push(w);
-                nd.finish = std::max(nd.finish, mma + nd.kt + 1.0);
-                TcUnit u{};
-                u.task = t;
-                u.col = c;
-                u.ktiles = nd.kt;
-                u.chain = 0;
-                u.dep0 = nd.dep.size() > 0 ? nodes[nd.dep[0]].ctr + c : -1;
-                u.dep1 = nd.dep.size() > 1 ? nodes[nd.dep[1]].ctr + c : -1;
-                u.need = need;
-                u.sig = nd.ctr >= 0 ? nd.ctr + c : -1;
-                units.push_back(u);
-            }
-        for (int cn : nd.cons) {
-            Node &cd = nodes[cn];
-            cd.ready = std::max(cd.ready, nd.finish);
-            if (--cd.unplaced == 0) waiting.push(cn);
-        }
-    }
-    return 1;
+    return dataflow_schedule(nodes, pair ? sm_count() / 2 : sm_count(), units, ndeps);
 }
 
 // Work units of every TC op for this entry's nrhs and column-tile choices.
@@ -2853,3 +2878,65 @@ int batch_tuned_widths(const Batch *b, int *widths, int cap)
 }
 
 }  // namespace mxb
+
+// Test hook (no counterpart in the reference): the unit order of a chained sweep, as the dataflow
+// launches use it, for a synthetic dependency forest; host code only.
+extern "C" int32_t mxb_debug_dataflow_order(int32_t nnodes, const int32_t *dep_first, const int32_t *deps,
+                                            const int32_t *ntask, const int32_t *kt, int32_t ncol, int32_t workers,
+                                            int32_t *node, int32_t *col, int32_t *dep0, int32_t *dep1,
+                                            int32_t *need, int32_t *sig, int64_t cap, int64_t *count)
+{
+    if (nnodes < 1 || !dep_first || !ntask || !kt || ncol < 1 || workers < 1 || !node || !col || !dep0 || !dep1 ||
+        !need || !sig || !count || cap < 0) {
+        mxb::set_error("bad dataflow-order arguments");
+        return MXB_ERR_ARG;
+    }
+    std::vector<mxb::DfNode> nodes(nnodes);
+    int task = 0;
+    for (int n = 0; n < nnodes; ++n) {
+        mxb::DfNode &nd = nodes[n];
+        if (ntask[n] < 1 || kt[n] < 0 || dep_first[n + 1] < dep_first[n] || (dep_first[n + 1] > dep_first[n] && !deps)) {
+            mxb::set_error("bad dataflow-order node");
+            return MXB_ERR_ARG;
+        }
+        nd.key = n;
+        nd.ncol = ncol;
+        nd.kt = kt[n];
+        for (int t = 0; t < ntask[n]; ++t) nd.tasks.push_back(task++);
+        for (int q = dep_first[n]; q < dep_first[n + 1]; ++q) nd.dep.push_back(deps[q]);
+    }
+    // levels as the sweeps number them: every node after the nodes it reads
+    for (int pass = 0; pass < nnodes; ++pass) {
+        bool moved = false;
+        for (mxb::DfNode &nd : nodes)
+            for (int d : nd.dep)
+                if (d >= 0 && d < nnodes && nodes[d].level + 1 > nd.level) {
+                    nd.level = nodes[d].level + 1;
+                    moved = true;
+                }
+        if (!moved) break;
+    }
+    std::vector<mxb::TcUnit> units;
+    std::vector<int> unit_node;
+    int ndeps = 0;
+    const int rc = mxb::dataflow_schedule(nodes, workers, units, ndeps, &unit_node);
+    if (rc < 0) return rc;
+    if (rc == 0) {
+        mxb::set_error("the dependencies are not a tree");
+        return MXB_ERR_UNSUPPORTED;
+    }
+    *count = (int64_t)units.size();
+    if ((int64_t)units.size() > cap) {
+        mxb::set_error("output arrays too short");
+        return MXB_ERR_ARG;
+    }
+    for (size_t u = 0; u < units.size(); ++u) {
+        node[u] = unit_node[u];
+        col[u] = units[u].col;
+        dep0[u] = units[u].dep0;
+        dep1[u] = units[u].dep1;
+        need[u] = units[u].need;
+        sig[u] = units[u].sig;
+    }
+    return MXB_OK;
+}
