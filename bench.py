@@ -517,7 +517,7 @@ def run_reference(args, cfg, rank):
         "impl": "reference", "metric": METRIC, "value": round(ms, 3), "unit": "ms", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": dict(WORKLOAD, flops_per_eval=flops, inputs="larger than L2 (W 512 MiB, CDS > 2 GiB)"),
+        "config": dict(cfg, flops_per_eval=flops, inputs="larger than L2 (W 512 MiB, CDS > 2 GiB)"),
         "gflops": round(flops / (ms * 1e-3) / 1e9, 2),
         "cpu_baseline": {"value": round(ms, 3), "unit": "ms", "cores": cores, "kind": "reference",
                          "sample": f"full workload per step ({r} rhs), median of {args.steps}; CBHGEMM "
