@@ -55,3 +55,26 @@ def test_built_for_sm100a(lib_path):
         pytest.skip("cuobjdump not available")
     out = subprocess.run([cuobjdump, "--list-elf", lib_path], capture_output=True, text=True).stdout
     assert "sm_100a" in out
+
+
+def test_binding_constants_match_header():
+    """The Python binding's constants are the header's #defines (error codes, precision modes and
+    flags, test hooks, tile and phase codes)."""
+    import re
+    text = open(_lib.HEADER).read()
+    defines = {m.group(1): int(m.group(2), 0)
+               for m in re.finditer(r"#define\s+(MXB_[A-Z0-9_]+)\s+\(?(-?(?:0x)?[0-9A-Fa-f]+)\)?", text)}
+    pairs = {
+        "MXB_OK": _lib.MXB_OK, "MXB_ERR_ARG": _lib.MXB_ERR_ARG, "MXB_ERR_STRUCTURE": _lib.MXB_ERR_STRUCTURE,
+        "MXB_ERR_CUDA": _lib.MXB_ERR_CUDA, "MXB_ERR_NOMEM": _lib.MXB_ERR_NOMEM, "MXB_ERR_TIMEOUT": _lib.MXB_ERR_TIMEOUT,
+        "MXB_ERR_UNSUPPORTED": _lib.MXB_ERR_UNSUPPORTED, "MXB_CACHE_SAMPLED": _lib.MXB_CACHE_SAMPLED,
+        "MXB_CACHE_FULL": _lib.MXB_CACHE_FULL, "MXB_CACHE_OFF": _lib.MXB_CACHE_OFF, "MXB_PREC_FP64": _lib.PREC_FP64,
+        "MXB_PREC_SPLIT_BF16": _lib.PREC_SPLIT_BF16, "MXB_PREC_SPLIT_BF16_FAR6": _lib.PREC_SPLIT_BF16_FAR6,
+        "MXB_PREC_SPLIT_BF16_X6": _lib.PREC_SPLIT_BF16_X6, "MXB_PLAN_ADJOINT": _lib.PLAN_ADJOINT,
+        "MXB_TILE_PAIR": _lib.TILE_PAIR, "MXB_DEBUG_STALL_ONE_WAIT": _lib.DEBUG_STALL_ONE_WAIT,
+        "MXB_DEBUG_CHAIN_LEVELS": _lib.DEBUG_CHAIN_LEVELS, "MXB_DEBUG_STALL_LEVEL": _lib.DEBUG_STALL_LEVEL,
+        "MXB_DEBUG_ONE_LAUNCH": _lib.DEBUG_ONE_LAUNCH,
+    }
+    missing = [k for k in pairs if k not in defines]
+    assert not missing, missing
+    assert {k: defines[k] for k in pairs} == pairs
