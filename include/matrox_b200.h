@@ -246,7 +246,10 @@ MXB_API int32_t mxb_plan_evaluate(mxb_plan *plan, const double *dW, double *dY, 
                           const int32_t *wptr, const int32_t *uptr, int32_t accumulate,
                           void *stream);
 /* dGW (+)= K~^T dG by the transposed traversal (no counterpart in the reference).  FP64 plans,
- * and split-BF16 plans created with MXB_PLAN_ADJOINT (MXB_ERR_UNSUPPORTED otherwise). */
+ * and split-BF16 plans created with MXB_PLAN_ADJOINT (MXB_ERR_UNSUPPORTED otherwise).
+ * A plan's evaluations and adjoints share its device workspaces: calls on one plan that overlap
+ * on the GPU (different streams without ordering between them) race; order them or use one
+ * stream, or one plan per stream. */
 MXB_API int32_t mxb_plan_adjoint(mxb_plan *plan, const double *dG, double *dGW, int32_t nrhs,
                          const int32_t *gptr, const int32_t *gwptr, int32_t accumulate,
                          void *stream);
